@@ -1,0 +1,108 @@
+/*
+ * model_mosaic_b200 C-ABI: the forward-model hot path of model_mosaic on one
+ * B200 (sm_100a).  Plain pointers and sizes only; every compute call takes
+ * device pointers and a cudaStream_t passed as `void*` (NULL = legacy default
+ * stream) and returns MM_OK (0) or a negative MM_E* status.  No call aborts
+ * the process; the text of the last error on the calling thread is returned
+ * by mm_last_error().  A handle is not thread-safe: use one per host thread.
+ * Handles own their workspace; the caller owns every array it passes.
+ *
+ * Array layouts are the reference's (C order):
+ *   obj  (nz, n, n)        float32          TomoReal.R input / RT output
+ *   sino (ntheta, nz, n)   float32|complex64 TomoReal.R output / RT input
+ *   psi  (ntheta, nz, n)   complex64        Propagation.D input / output
+ */
+#ifndef MODEL_MOSAIC_B200_MOSAIC_H
+#define MODEL_MOSAIC_B200_MOSAIC_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MM_OK         0
+#define MM_EINVAL    -1   /* bad argument / unsupported size */
+#define MM_ENOMEM    -2   /* device allocation failed */
+#define MM_ECUDA     -3   /* CUDA runtime error */
+#define MM_ECUFFT    -4   /* cuFFT error */
+#define MM_ETIMEOUT  -5   /* a bounded device wait gave up */
+
+#define MM_F32 0
+#define MM_C64 1
+
+typedef struct mm_tomo mm_tomo;
+typedef struct mm_prop mm_prop;
+
+/* USFFT options.  Zero-initialised fields take the reference defaults
+ * (processing/tomo.py:39-42): eps = 1e-3, m from eps (m = 4), oversampling 2. */
+typedef struct mm_tomo_opts {
+    double eps;        /* Gaussian accuracy; <= 0 -> 1e-3 */
+    int    m;          /* half-width override; <= 0 -> from eps (reference formula) */
+    int    clamp_xy;   /* 1: clamp sample coordinates to [-1/2, 1/2 - 1e-5] in R as
+                          TomoLargeReal's gather does (processing/kernels.py:478-481) */
+    int    reserved[5];
+} mm_tomo_opts;
+
+/* Library and error reporting. */
+int         mm_version(void);
+int         mm_last_error(char* buf, size_t len);  /* copies the message, returns its length */
+
+/* ---- USFFT Radon pair ---------------------------------------------------
+ * mm_tomo_create replaces TomoReal.__init__(n, nz, theta)
+ *   (processing/tomo.py:30-88) and TomoLargeReal.__init__(n, theta, chunk_xy)
+ *   (processing/tomo_large.py:72-148).  theta_host: ntheta float32 radians.
+ *   opts may be NULL (reference defaults).  n must be even, 8 <= n <= 16384. */
+int mm_tomo_create(int n, int nz, int ntheta, const float* theta_host,
+                   const mm_tomo_opts* opts, mm_tomo** out);
+/* Replaces TomoReal.free (processing/tomo.py:109-119) / TomoLargeReal.free. */
+int mm_tomo_destroy(mm_tomo* h);
+
+/* Replaces TomoReal.R (processing/tomo.py:121-151) and TomoLargeReal.R
+ *   (processing/tomo_large.py:344-368): obj (nz, n, n) f32 -> sino
+ *   (ntheta, nz, n) f32, for 1 <= nz <= the handle's nz.  Device pointers. */
+int mm_tomo_R(mm_tomo* h, const float* obj, float* sino, int nz, void* stream);
+
+/* Replaces TomoReal.RT (processing/tomo.py:153-188) and TomoLargeReal.RT
+ *   (processing/tomo_large.py:582-630): sino (ntheta, nz, n) of `dtype`
+ *   (MM_F32 or MM_C64) -> obj (nz, n, n) of the same dtype (real part only
+ *   for MM_F32, as the reference).  Deterministic: no float atomics. */
+int mm_tomo_RT(mm_tomo* h, const void* sino, int dtype, void* obj, int nz, void* stream);
+
+/* Builds the adjoint's static scatter table now instead of on the first RT
+ * call (the reference defers its RT buffers the same way, tomo.py:90-107). */
+int mm_tomo_prepare_rt(mm_tomo* h, void* stream);
+
+/* Bytes of device workspace the handle holds now. */
+size_t mm_tomo_workspace_bytes(const mm_tomo* h);
+
+/* ---- Fresnel propagator -------------------------------------------------
+ * mm_prop_create replaces Propagation.__init__(n, nz, ntheta, ndist,
+ *   wavelength, voxelsize, distance) (processing/propagation.py:18-35) and
+ *   PropagationLarge.__init__ (processing/propagation_large.py:55-94).
+ *   2n and 2nz must be powers of two in [4, 4096]. */
+int mm_prop_create(int n, int nz, int ntheta, int ndist, double wavelength,
+                   double voxelsize, const double* distance_host, mm_prop** out);
+int mm_prop_destroy(mm_prop* h);
+
+/* Replaces Propagation.D (processing/propagation.py:47-64) and
+ *   PropagationLarge.D (processing/propagation_large.py:202-236):
+ *   psi (ntheta, nz, n) c64 -> out (ntheta, nz, n) c64, distance index j.
+ *   psi and out may alias. */
+int mm_prop_D(mm_prop* h, const void* psi, void* out, int ntheta, int j, void* stream);
+
+/* Adjoint of D (no reference counterpart: the reference ships only D,
+ *   processing/propagation_large.py:15).  Same layouts as mm_prop_D. */
+int mm_prop_DT(mm_prop* h, const void* g, void* out, int ntheta, int j, void* stream);
+
+/* step3_propagation.py:218-225 fused: proj (ntheta, nz, n) f32 ->
+ *   psi = exp(-p*s/beta_r) (cos p*s, sin p*s) with s = inv_norm,
+ *   1/beta_r = inv_beta_ratio (_psi_from_proj, :94-103) -> D -> |.|^2
+ *   (_abs2_c64_to_f32, :105-110) -> intensity (ntheta, nz, n) f32. */
+int mm_prop_intensity(mm_prop* h, const float* proj, float inv_norm, float inv_beta_ratio,
+                      float* intensity, int ntheta, int j, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

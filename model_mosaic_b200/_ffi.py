@@ -1,0 +1,89 @@
+"""ctypes binding of the C-ABI in include/mosaic.h (``libmosaic.so``).
+
+The shared library is built in-tree by ``model_mosaic_b200/build.py``.  There
+is no fallback: if the library is missing or fails to load, every operator
+raises at construction time.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmosaic.so")
+
+MM_OK, MM_EINVAL, MM_ENOMEM, MM_ECUDA, MM_ECUFFT, MM_ETIMEOUT = 0, -1, -2, -3, -4, -5
+MM_F32, MM_C64 = 0, 1
+
+_lib = None
+_lock = threading.Lock()
+
+
+class MosaicError(RuntimeError):
+    """A C-ABI call returned a CUDA/cuFFT failure status."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[status {status}] {msg}")
+        self.status = status
+
+
+class MosaicTimeout(MosaicError):
+    pass
+
+
+def _declare(L):
+    p, i, f, d, sz = C.c_void_p, C.c_int, C.c_float, C.c_double, C.c_size_t
+    L.mm_version.restype = i
+    L.mm_last_error.argtypes = [C.c_char_p, sz]
+    L.mm_last_error.restype = i
+    L.mm_tomo_create.argtypes = [i, i, i, p, p, C.POINTER(p)]
+    L.mm_tomo_destroy.argtypes = [p]
+    L.mm_tomo_R.argtypes = [p, p, p, i, p]
+    L.mm_tomo_RT.argtypes = [p, p, i, p, i, p]
+    L.mm_tomo_prepare_rt.argtypes = [p, p]
+    L.mm_tomo_workspace_bytes.argtypes = [p]
+    L.mm_tomo_workspace_bytes.restype = sz
+    L.mm_prop_create.argtypes = [i, i, i, i, d, d, p, C.POINTER(p)]
+    L.mm_prop_destroy.argtypes = [p]
+    L.mm_prop_D.argtypes = [p, p, p, i, i, p]
+    L.mm_prop_DT.argtypes = [p, p, p, i, i, p]
+    L.mm_prop_intensity.argtypes = [p, p, f, f, p, i, i, p]
+    for name in ("mm_tomo_create", "mm_tomo_destroy", "mm_tomo_R", "mm_tomo_RT", "mm_tomo_prepare_rt",
+                 "mm_prop_create", "mm_prop_destroy", "mm_prop_D", "mm_prop_DT", "mm_prop_intensity"):
+        getattr(L, name).restype = i
+    return L
+
+
+def lib():
+    """Load libmosaic.so once; raise if it is absent (no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not os.path.exists(LIB_PATH):
+                    raise RuntimeError(
+                        f"{LIB_PATH} not found: build it with `python -m model_mosaic_b200.build` "
+                        "(the CUDA library is required; there is no CPU path)")
+                _lib = _declare(C.CDLL(LIB_PATH))
+    return _lib
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    lib().mm_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int, what: str = "") -> None:
+    """Turn a C-ABI status into a Python exception (never aborts)."""
+    if status == MM_OK:
+        return
+    msg = last_error() or what
+    if status == MM_EINVAL:
+        raise ValueError(msg)
+    if status == MM_ENOMEM:
+        raise MemoryError(msg)
+    if status == MM_ETIMEOUT:
+        raise MosaicTimeout(status, msg)
+    raise MosaicError(status, msg)

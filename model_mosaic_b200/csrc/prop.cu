@@ -1,0 +1,403 @@
+// Fresnel propagator D and its adjoint DT for sm_100a.
+//
+// Reference (processing/propagation.py:18-64, processing/kernels.py:530-550):
+//   D(psi) = crop( IFFT2_unnorm( fker_j * FFT2( mirrorpad(psi) ) ) ),
+//   fker_j = exp(-i pi lambda z_j (fx^2 + fy^2)) / (4 n nz).
+// The chirp separates, K = Kx(fx) Ky(fy) (processing/propagation_large.py:7-13),
+// and the y and x halves commute, so D runs as two passes over HBM:
+//   y-pass  per column: mirror-pad to 2nz, FFT, *Ky/(2nz), IFFT, crop  -> mid
+//   x-pass  per row:    mirror-pad to 2n,  FFT, *Kx/(2n),  IFFT, crop  -> out
+// Each pass keeps its column/row in registers and shared memory
+// (fft_smem.cuh): 24 bytes of HBM traffic per pixel for f32 in, c64 mid,
+// f32 out.  psi = exp(-p s/beta_r) (cos p s, sin p s) (step3_propagation.py:
+// 94-103) is built in the y-pass load and |u|^2 (:105-110) in the x-pass
+// store.  The chirp phase is evaluated in FP64 and reduced mod 2 pi.
+// DT is the exact adjoint: zero-embed, FFT, *conj(K), IFFT, fold the mirrored
+// borders back onto their source pixels.
+#include "mm_common.cuh"
+#include "fft_smem.cuh"
+
+#include <math.h>
+
+#include <vector>
+
+using mm::dev_alloc;
+using mmfft::cmul;
+using mmfft::cmulc;
+using mmfft::reg_fft;
+using mmfft::Split;
+
+struct mm_prop {
+    int n = 0, nz = 0, ntheta = 0, ndist = 0;
+    float2* Kx = nullptr;   // (ndist, 2n)
+    float2* Ky = nullptr;   // (ndist, 2nz)
+    float2* twx = nullptr;  // (2n)  exp(-2 pi i k / 2n)
+    float2* twy = nullptr;  // (2nz)
+    float2* mid = nullptr;  // (ntheta, nz, n)
+    size_t ws_bytes = 0;
+};
+
+namespace {
+
+// Source index of padded position t (processing/kernels.py:541-544).
+__device__ __forceinline__ int mirror_src(int t, int len) {
+    const int h = len / 2;
+    return t < h ? h - t - 1 : (t >= len + h ? 2 * len - t + h - 1 : t - h);
+}
+// The second padded position that folds onto pixel r (the first is r + len/2).
+__device__ __forceinline__ int mirror_partner(int r, int len) {
+    const int h = len / 2;
+    return r < h ? h - 1 - r : 2 * len + h - 1 - r;
+}
+
+// ---------------------------------------------------------------- y-pass
+// IN: 0 complex psi, 1 real projection (psi built on load).  Block (CW, R2):
+// lanes run over CW adjacent columns, threadIdx.y over the R2 sub-sequences.
+template <int L, int CW, int IN, bool ADJ>
+__global__ void __launch_bounds__(CW * Split<L>::R2) k_ypass(const void* __restrict__ src, float2* __restrict__ dst,
+                                                            const float2* __restrict__ Ky,
+                                                            const float2* __restrict__ tw, int n, int nz,
+                                                            float s, float ib) {
+    constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2;
+    extern __shared__ float2 sm[];  // [R1][R2][CW]
+    const int c = threadIdx.x, g = threadIdx.y;
+    const int x = blockIdx.x * CW + c;
+    const bool live = x < n;
+    const long plane = (long)blockIdx.y * nz * n;
+    float2 v[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) {
+        const int idx = R2 * n1 + g;
+        int r;
+        bool zero = false;
+        if (!ADJ) {
+            r = mirror_src(idx, nz);
+        } else {
+            r = idx - nz / 2;
+            zero = r < 0 || r >= nz;
+        }
+        float2 a = make_float2(0.f, 0.f);
+        if (live && !zero) {
+            const long off = plane + (long)r * n + x;
+            if (IN == 0) {
+                a = __ldg(static_cast<const float2*>(src) + off);
+            } else {
+                const float ph = __ldg(static_cast<const float*>(src) + off) * s;
+                const float at = expf(-ph * ib);
+                float sn, cs;
+                sincosf(ph, &sn, &cs);
+                a = make_float2(at * cs, at * sn);
+            }
+        }
+        v[n1] = a;
+    }
+    reg_fft<R1, false>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < R1; ++k1)
+        if (g) v[k1] = cmul(v[k1], __ldg(tw + g * k1));
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) sm[(k1 * R2 + g) * CW + c] = v[k1];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < R1 / R2; ++i) {
+        const int k1 = g + R2 * i;
+        float2 u[R2];
+#pragma unroll
+        for (int n2 = 0; n2 < R2; ++n2) u[n2] = sm[(k1 * R2 + n2) * CW + c];
+        reg_fft<R2, false>(u);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) {
+            const float2 K = __ldg(Ky + k1 + R1 * k2);
+            u[k2] = ADJ ? cmulc(u[k2], K) : cmul(u[k2], K);
+        }
+        reg_fft<R2, true>(u);
+#pragma unroll
+        for (int m2 = 1; m2 < R2; ++m2)
+            if (k1) u[m2] = cmulc(u[m2], __ldg(tw + k1 * m2));
+#pragma unroll
+        for (int m2 = 0; m2 < R2; ++m2) sm[(k1 * R2 + m2) * CW + c] = u[m2];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) v[k1] = sm[(k1 * R2 + g) * CW + c];
+    reg_fft<R1, true>(v);
+    if (!ADJ) {
+#pragma unroll
+        for (int m1 = 0; m1 < R1; ++m1) {
+            const int r = g + R2 * m1 - nz / 2;
+            if (live && r >= 0 && r < nz) dst[plane + (long)r * n + x] = v[m1];
+        }
+    } else {
+        __syncthreads();
+#pragma unroll
+        for (int m1 = 0; m1 < R1; ++m1) sm[(g + R2 * m1) * CW + c] = v[m1];
+        __syncthreads();
+        for (int r = g; r < nz; r += R2) {
+            const float2 a = sm[(r + nz / 2) * CW + c], b = sm[mirror_partner(r, nz) * CW + c];
+            if (live) dst[plane + (long)r * n + x] = make_float2(a.x + b.x, a.y + b.y);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- x-pass
+// OUT: 0 complex, 1 |.|^2 float.  Block (R2, RPB): R2 threads per row.
+template <int L, int RPB, int OUT, bool ADJ>
+__global__ void __launch_bounds__(RPB * Split<L>::R2) k_xpass(const float2* __restrict__ src, void* __restrict__ dst,
+                                                             const float2* __restrict__ Kx,
+                                                             const float2* __restrict__ tw, int n, long rows) {
+    constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2, P = R2 + 1;
+    extern __shared__ float2 sm[];  // [RPB][R1][R2 + 1]
+    const int g = threadIdx.x, rr = threadIdx.y;
+    const long row = (long)blockIdx.x * RPB + rr;
+    const bool live = row < rows;
+    float2* S = sm + rr * R1 * P;
+    const float2* in = src + row * n;
+    float2 v[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) {
+        const int idx = R2 * n1 + g;
+        int col;
+        bool zero = false;
+        if (!ADJ) {
+            col = mirror_src(idx, n);
+        } else {
+            col = idx - n / 2;
+            zero = col < 0 || col >= n;
+        }
+        v[n1] = (live && !zero) ? __ldg(in + col) : make_float2(0.f, 0.f);
+    }
+    reg_fft<R1, false>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < R1; ++k1)
+        if (g) v[k1] = cmul(v[k1], __ldg(tw + g * k1));
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) S[k1 * P + g] = v[k1];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < R1 / R2; ++i) {
+        const int k1 = g + R2 * i;
+        float2 u[R2];
+#pragma unroll
+        for (int n2 = 0; n2 < R2; ++n2) u[n2] = S[k1 * P + n2];
+        reg_fft<R2, false>(u);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) {
+            const float2 K = __ldg(Kx + k1 + R1 * k2);
+            u[k2] = ADJ ? cmulc(u[k2], K) : cmul(u[k2], K);
+        }
+        reg_fft<R2, true>(u);
+#pragma unroll
+        for (int m2 = 1; m2 < R2; ++m2)
+            if (k1) u[m2] = cmulc(u[m2], __ldg(tw + k1 * m2));
+#pragma unroll
+        for (int m2 = 0; m2 < R2; ++m2) S[k1 * P + m2] = u[m2];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) v[k1] = S[k1 * P + g];
+    reg_fft<R1, true>(v);
+    if (!ADJ) {
+#pragma unroll
+        for (int m1 = 0; m1 < R1; ++m1) {
+            const int c = g + R2 * m1 - n / 2;
+            if (live && c >= 0 && c < n) {
+                if (OUT == 0)
+                    static_cast<float2*>(dst)[row * n + c] = v[m1];
+                else
+                    static_cast<float*>(dst)[row * n + c] = v[m1].x * v[m1].x + v[m1].y * v[m1].y;
+            }
+        }
+    } else {
+        __syncthreads();
+#pragma unroll
+        for (int m1 = 0; m1 < R1; ++m1) S[g + R2 * m1] = v[m1];   // L <= R1 * P
+        __syncthreads();
+        for (int c = g; c < n; c += R2) {
+            const float2 a = S[c + n / 2], b = S[mirror_partner(c, n)];
+            if (live) static_cast<float2*>(dst)[row * n + c] = make_float2(a.x + b.x, a.y + b.y);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- launch
+template <int L, int IN, bool ADJ>
+int launch_y(const mm_prop* h, const void* src, int ntheta, int j, float s, float ib, cudaStream_t st) {
+    constexpr int R2 = Split<L>::R2;
+    constexpr int CW0 = 256 / R2;
+    constexpr int CW = CW0 < 4 ? 4 : (CW0 > 32 ? 32 : CW0);
+    const size_t smem = (size_t)L * CW * sizeof(float2);
+    auto kern = k_ypass<L, CW, IN, ADJ>;
+    MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 block(CW, R2), grid((h->n + CW - 1) / CW, ntheta);
+    kern<<<grid, block, smem, st>>>(src, h->mid, h->Ky + (size_t)j * 2 * h->nz, h->twy, h->n, h->nz, s, ib);
+    MM_LAUNCHED();
+    return MM_OK;
+}
+
+template <int L, int OUT, bool ADJ>
+int launch_x(const mm_prop* h, void* dst, int ntheta, int j, cudaStream_t st) {
+    constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2;
+    constexpr int RPB = R2 >= 128 ? 1 : 128 / R2;
+    const size_t smem = (size_t)RPB * R1 * (R2 + 1) * sizeof(float2);
+    auto kern = k_xpass<L, RPB, OUT, ADJ>;
+    MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const long rows = (long)ntheta * h->nz;
+    dim3 block(R2, RPB), grid((unsigned)((rows + RPB - 1) / RPB));
+    kern<<<grid, block, smem, st>>>(h->mid, dst, h->Kx + (size_t)j * 2 * h->n, h->twx, h->n, rows);
+    MM_LAUNCHED();
+    return MM_OK;
+}
+
+template <int IN, bool ADJ>
+int dispatch_y(const mm_prop* h, const void* src, int ntheta, int j, float s, float ib, cudaStream_t st) {
+    switch (2 * h->nz) {
+        case 4: return launch_y<4, IN, ADJ>(h, src, ntheta, j, s, ib, st);
+        case 8: return launch_y<8, IN, ADJ>(h, src, ntheta, j, s, ib, st);
+        case 16: return launch_y<16, IN, ADJ>(h, src, ntheta, j, s, ib, st);
+        case 32: return launch_y<32, IN, ADJ>(h, src, ntheta, j, s, ib, st);
+        case 64: return launch_y<64, IN, ADJ>(h, src, ntheta, j, s, ib, st);
+        case 128: return launch_y<128, IN, ADJ>(h, src, ntheta, j, s, ib, st);
+        case 256: return launch_y<256, IN, ADJ>(h, src, ntheta, j, s, ib, st);
+        case 512: return launch_y<512, IN, ADJ>(h, src, ntheta, j, s, ib, st);
+        case 1024: return launch_y<1024, IN, ADJ>(h, src, ntheta, j, s, ib, st);
+        case 2048: return launch_y<2048, IN, ADJ>(h, src, ntheta, j, s, ib, st);
+        case 4096: return launch_y<4096, IN, ADJ>(h, src, ntheta, j, s, ib, st);
+    }
+    MM_REQUIRE(false, "unsupported 2*nz=%d", 2 * h->nz);
+}
+
+template <int OUT, bool ADJ>
+int dispatch_x(const mm_prop* h, void* dst, int ntheta, int j, cudaStream_t st) {
+    switch (2 * h->n) {
+        case 4: return launch_x<4, OUT, ADJ>(h, dst, ntheta, j, st);
+        case 8: return launch_x<8, OUT, ADJ>(h, dst, ntheta, j, st);
+        case 16: return launch_x<16, OUT, ADJ>(h, dst, ntheta, j, st);
+        case 32: return launch_x<32, OUT, ADJ>(h, dst, ntheta, j, st);
+        case 64: return launch_x<64, OUT, ADJ>(h, dst, ntheta, j, st);
+        case 128: return launch_x<128, OUT, ADJ>(h, dst, ntheta, j, st);
+        case 256: return launch_x<256, OUT, ADJ>(h, dst, ntheta, j, st);
+        case 512: return launch_x<512, OUT, ADJ>(h, dst, ntheta, j, st);
+        case 1024: return launch_x<1024, OUT, ADJ>(h, dst, ntheta, j, st);
+        case 2048: return launch_x<2048, OUT, ADJ>(h, dst, ntheta, j, st);
+        case 4096: return launch_x<4096, OUT, ADJ>(h, dst, ntheta, j, st);
+    }
+    MM_REQUIRE(false, "unsupported 2*n=%d", 2 * h->n);
+}
+
+int check_call(const mm_prop* h, const void* a, const void* b, int ntheta, int j, const char* who) {
+    MM_REQUIRE(h != nullptr, "%s: NULL handle", who);
+    MM_REQUIRE(a != nullptr && b != nullptr, "%s: NULL array", who);
+    MM_REQUIRE(ntheta >= 1 && ntheta <= h->ntheta, "%s: ntheta=%d outside [1, %d]", who, ntheta, h->ntheta);
+    MM_REQUIRE(j >= 0 && j < h->ndist, "%s: distance index %d outside [0, %d)", who, j, h->ndist);
+    return MM_OK;
+}
+
+void destroy(mm_prop* h) {
+    void* bufs[] = {h->Kx, h->Ky, h->twx, h->twy, h->mid};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    delete h;
+}
+
+// exp(-i pi lambda z f^2) / len for the float32 fftfreq grid of `len` points
+// (processing/propagation.py:23-31), phase in FP64 reduced mod 2 pi.
+void chirp(std::vector<float2>& out, int len, double voxelsize, double wavelength, double z) {
+    const double val = 1.0 / (len * voxelsize);
+    for (int k = 0; k < len; ++k) {
+        const int kk = k < (len + 1) / 2 ? k : k - len;
+        const double f = (double)(float)(kk * val);
+        double ph = fmod(M_PI * wavelength * z * f * f, 2.0 * M_PI);
+        out[k] = make_float2((float)(cos(-ph) / len), (float)(sin(-ph) / len));
+    }
+}
+
+void twiddles(std::vector<float2>& out, int len) {
+    for (int k = 0; k < len; ++k) {
+        const double a = -2.0 * M_PI * k / len;
+        out[k] = make_float2((float)cos(a), (float)sin(a));
+    }
+}
+
+}  // namespace
+
+extern "C" int mm_prop_create(int n, int nz, int ntheta, int ndist, double wavelength, double voxelsize,
+                              const double* distance_host, mm_prop** out) {
+    MM_REQUIRE(out != nullptr, "mm_prop_create: out is NULL");
+    *out = nullptr;
+    MM_REQUIRE(mm_is_pow2(2L * n) && 2 * n >= 4 && 2 * n <= 4096,
+               "mm_prop_create: 2n=%d must be a power of two in [4, 4096]", 2 * n);
+    MM_REQUIRE(mm_is_pow2(2L * nz) && 2 * nz >= 4 && 2 * nz <= 4096,
+               "mm_prop_create: 2nz=%d must be a power of two in [4, 4096]", 2 * nz);
+    MM_REQUIRE(ntheta >= 1 && ndist >= 1 && distance_host != nullptr, "mm_prop_create: bad ntheta/ndist");
+    MM_REQUIRE(voxelsize > 0, "mm_prop_create: voxelsize must be positive");
+    MM_CUDA(mmfft::init_constants());
+    mm_prop* h = new mm_prop();
+    h->n = n;
+    h->nz = nz;
+    h->ntheta = ntheta;
+    h->ndist = ndist;
+    std::vector<float2> kx((size_t)ndist * 2 * n), ky((size_t)ndist * 2 * nz), tx(2 * n), ty(2 * nz), tmp;
+    for (int j = 0; j < ndist; ++j) {
+        tmp.assign(2 * n, make_float2(0, 0));
+        chirp(tmp, 2 * n, voxelsize, wavelength, distance_host[j]);
+        std::copy(tmp.begin(), tmp.end(), kx.begin() + (size_t)j * 2 * n);
+        tmp.assign(2 * nz, make_float2(0, 0));
+        chirp(tmp, 2 * nz, voxelsize, wavelength, distance_host[j]);
+        std::copy(tmp.begin(), tmp.end(), ky.begin() + (size_t)j * 2 * nz);
+    }
+    twiddles(tx, 2 * n);
+    twiddles(ty, 2 * nz);
+    struct B { float2** p; const std::vector<float2>* v; const char* what; } bs[] = {
+        {&h->Kx, &kx, "x chirp"}, {&h->Ky, &ky, "y chirp"}, {&h->twx, &tx, "x twiddles"}, {&h->twy, &ty, "y twiddles"}};
+    for (auto& b : bs) {
+        int rc = dev_alloc((void**)b.p, b.v->size() * sizeof(float2), b.what);
+        if (rc != MM_OK) {
+            destroy(h);
+            return rc;
+        }
+        h->ws_bytes += b.v->size() * sizeof(float2);
+        if (cudaMemcpy(*b.p, b.v->data(), b.v->size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess) {
+            mm::set_error("mm_prop_create: table upload failed");
+            destroy(h);
+            return MM_ECUDA;
+        }
+    }
+    const size_t mid = (size_t)ntheta * nz * n;
+    int rc = dev_alloc((void**)&h->mid, mid * sizeof(float2), "propagator intermediate");
+    if (rc != MM_OK) {
+        destroy(h);
+        return rc;
+    }
+    h->ws_bytes += mid * sizeof(float2);
+    *out = h;
+    return MM_OK;
+}
+
+extern "C" int mm_prop_destroy(mm_prop* h) {
+    if (!h) return MM_OK;
+    cudaDeviceSynchronize();
+    destroy(h);
+    return MM_OK;
+}
+
+extern "C" int mm_prop_D(mm_prop* h, const void* psi, void* out, int ntheta, int j, void* stream) {
+    MM_TRY(check_call(h, psi, out, ntheta, j, "mm_prop_D"));
+    cudaStream_t st = (cudaStream_t)stream;
+    MM_TRY((dispatch_y<0, false>(h, psi, ntheta, j, 0.f, 0.f, st)));
+    return dispatch_x<0, false>(h, out, ntheta, j, st);
+}
+
+extern "C" int mm_prop_DT(mm_prop* h, const void* g, void* out, int ntheta, int j, void* stream) {
+    MM_TRY(check_call(h, g, out, ntheta, j, "mm_prop_DT"));
+    cudaStream_t st = (cudaStream_t)stream;
+    MM_TRY((dispatch_y<0, true>(h, g, ntheta, j, 0.f, 0.f, st)));
+    return dispatch_x<0, true>(h, out, ntheta, j, st);
+}
+
+extern "C" int mm_prop_intensity(mm_prop* h, const float* proj, float inv_norm, float inv_beta_ratio,
+                                 float* intensity, int ntheta, int j, void* stream) {
+    MM_TRY(check_call(h, proj, intensity, ntheta, j, "mm_prop_intensity"));
+    cudaStream_t st = (cudaStream_t)stream;
+    MM_TRY((dispatch_y<1, false>(h, proj, ntheta, j, inv_norm, inv_beta_ratio, st)));
+    return dispatch_x<1, false>(h, intensity, ntheta, j, st);
+}

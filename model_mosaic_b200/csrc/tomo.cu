@@ -1,0 +1,859 @@
+// USFFT Radon pair (TomoReal / TomoLargeReal .R and .RT) for sm_100a.
+//
+// Reference operator (processing/tomo.py:121-188, processing/kernels.py):
+//   R(obj)  = Re( c . IFFT_r( c . (1/n) G F2( pad2n(phi . obj) ) ) ) / 4
+//   RT(y)   = phi . crop( c2 . IFFT2( c2 . G^H( c . FFT_r(c . y) ) ) )
+// with G the (2m+1)^2 Gaussian gather onto the polar grid.
+//
+// B200 formulation (same operator, different schedule and layout):
+//  * Slices are interleaved in the spectrum: F[v][u][z] with z innermost, so
+//    one warp owns one polar sample for 32..64 slices; the Gaussian weights
+//    are computed once per sample and every tap is one coalesced 256/512-byte
+//    load.
+//  * Real input makes the spectrum and every polar line Hermitian, so only the
+//    n/2+1 samples with r >= 0 (plus r = -1/2) are gathered, samples with
+//    x0 < 0 are taken at -p and conjugated, and the r-IFFT + c1dfftshift +
+//    .real/4 collapse into one C2R of length n whose input index k holds
+//    sample j = (k + n/2) mod n with sign (-1)^j / (4 n^2).
+//  * RT is the exact transpose of that R.  The scatter is a pull over a
+//    static CSR table (destination cell -> (sample, weight, conj)) built once
+//    by a radix sort of (cell, sample, tap) keys: deterministic, no atomics.
+#include "mm_common.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
+#include <math.h>
+
+#include <algorithm>
+#include <vector>
+
+using mm::dev_alloc;
+
+struct mm_tomo {
+    int n = 0, nz = 0, ntheta = 0, m = 0, zs = 0, K = 0, clamp = 0;
+    float mu = 0.f, c0 = 0.f, c1 = 0.f, phi_scale = 0.f;
+    int device = 0;
+    float* d_cos = nullptr;
+    float* d_sin = nullptr;
+    float* d_phi1 = nullptr;
+    // forward buffers
+    float* P = nullptr;          // (zs, n, 2n)     padded phi*obj rows
+    float2* X = nullptr;         // (zs, n, n+1)    row spectra
+    float2* Y = nullptr;         // (2n, n+1, zs)   row spectra in centre rows, zero elsewhere
+    float2* F = nullptr;         // (2n, n+1, zs)   half spectrum, raw fftfreq order
+    float2* Hh = nullptr;        // (n/2+1, T, zs)  C2R input along r
+    float* sino_tmp = nullptr;   // (T, zs, n)      only when nz < zs
+    void* fft_work = nullptr;
+    size_t fft_work_bytes = 0;
+    cufftHandle plan_xr2c = 0, plan_xc2r = 0, plan_y = 0, plan_rc2r = 0, plan_rr2c = 0, plan_rc2c = 0;
+    bool plans_rt = false, plans_c = false;
+    bool y_dirty = false;        // RT used Y as scratch: its zero pad rows need restoring
+    // adjoint scatter table
+    bool csr_ready = false;
+    unsigned* csr_ptr = nullptr;  // ncells + 1
+    unsigned* csr_idx = nullptr;  // sample index (k*T + t) | conj << 31
+    float* csr_w = nullptr;
+    size_t nnz = 0;
+    float* ypad = nullptr;       // (T, zs, n) real sino padded in z (nz < zs)
+    float2* yc = nullptr;        // (T, zs, n) complex sino spectrum (complex RT)
+    size_t ws_bytes = 0;
+};
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// --------------------------------------------------------------------------
+// Sample geometry shared by the gather and the scatter-table builder.
+// Coordinates follow processing/kernels.py:293-299 in float32; cos/sin come
+// from an FP64 table.  Samples with x0 < 0 are taken at -p (Hermitian).
+struct SampleGeo {
+    int j, bx, by;
+    bool mir;
+    float x0, y0;
+};
+
+__device__ __forceinline__ SampleGeo sample_geo(int t, int k, int n, int M, const float* __restrict__ cosT,
+                                                const float* __restrict__ sinT, bool clamp = false) {
+    SampleGeo g;
+    g.j = (k < n / 2) ? k + n / 2 : 0;
+    const float cx = n * 0.5f;
+    const float r = ((float)g.j - cx) / (float)n;
+    float x0 = r * __ldg(cosT + t);
+    float y0 = -r * __ldg(sinT + t);
+    if (clamp) {  // TomoLargeReal's gather (processing/kernels.py:478-481)
+        x0 = fminf(fmaxf(x0, -0.5f), 0.5f - 1e-5f);
+        y0 = fminf(fmaxf(y0, -0.5f), 0.5f - 1e-5f);
+    }
+    g.mir = x0 < 0.f;
+    if (g.mir) {
+        x0 = -x0;
+        y0 = -y0;
+    }
+    const float ftwon = (float)(2 * n);
+    g.bx = __float2int_rn(ftwon * x0) - M;   // rintf: round half to even
+    g.by = __float2int_rn(ftwon * y0) - M;
+    g.x0 = x0;
+    g.y0 = y0;
+    return g;
+}
+
+// Gaussian weight of tap offset i along one axis; `sgn` folds the
+// (-1)^(k0+k1) shift of processing/kernels.py:319-321 in per axis.
+__device__ __forceinline__ float tap_weight(int ell, float pos, float inv_twon, float c1) {
+    const float w = (float)ell * inv_twon - pos;
+    const float e = expf(c1 * w * w);
+    return (ell & 1) ? -e : e;
+}
+
+// Destination of tap (u, v) in the stored half plane (columns 0..n, rows in
+// raw order): reflected through the origin when u is outside [0, n].
+__device__ __forceinline__ void tap_cell(int u, int v, int n, int& row, int& col, bool& cj) {
+    const int twon = 2 * n;
+    if (u >= 0 && u <= n) {
+        col = u;
+        cj = false;
+    } else {
+        col = (u < 0) ? -u : twon - u;
+        v = -v;
+        cj = true;
+    }
+    row = v < 0 ? v + twon : (v >= twon ? v - twon : v);
+}
+
+template <int ZV>
+struct ZVec;
+template <>
+struct ZVec<1> {
+    static __device__ __forceinline__ void load(const float2* p, float* v) {
+        float2 a = __ldg(p);
+        v[0] = a.x; v[1] = a.y;
+    }
+    static __device__ __forceinline__ void store(float2* p, const float* v) {
+        *p = make_float2(v[0], v[1]);
+    }
+};
+template <>
+struct ZVec<2> {
+    static __device__ __forceinline__ void load(const float2* p, float* v) {
+        float4 a = __ldg(reinterpret_cast<const float4*>(p));
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    }
+    static __device__ __forceinline__ void store(float2* p, const float* v) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+};
+
+// --------------------------------------------------------------------------
+// R stage 1: padded phi*obj rows (processing/tomo.py:129-132, x padding only;
+// the y padding lives in the zero rows of Y).
+__global__ void k_pad_phi(const float* __restrict__ obj, float* __restrict__ P,
+                          const float* __restrict__ phi1, float phis, int n, int nzc) {
+    const long row = blockIdx.x;          // z * n + y
+    const int y = (int)(row % n);
+    const int z = (int)(row / n);
+    const int twon = 2 * n, h = n / 2;
+    float* out = P + row * twon;
+    const bool live = z < nzc;
+    const float* src = obj + row * n;
+    const float py = phis * __ldg(phi1 + y);
+    for (int x2 = threadIdx.x; x2 < twon; x2 += blockDim.x) {
+        const int x = x2 - h;
+        float v = 0.f;
+        if (live && x >= 0 && x < n) v = py * __ldg(phi1 + x) * __ldg(src + x);
+        out[x2] = v;
+    }
+}
+
+// R stage 3: X[z][y][u] -> Y[n/2 + y][u][z]
+__global__ void k_transpose_in(const float2* __restrict__ X, float2* __restrict__ Y, int n, int zs) {
+    __shared__ float2 tile[32][33];
+    const int u0 = blockIdx.x * 32, z0 = blockIdx.y * 32, y = blockIdx.z;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int j = ty; j < 32; j += 8) {
+        const int z = z0 + j, u = u0 + tx;
+        if (z < zs && u <= n) tile[j][tx] = __ldg(X + ((long)z * n + y) * (n + 1) + u);
+    }
+    __syncthreads();
+    for (int j = ty; j < 32; j += 8) {
+        const int u = u0 + j, z = z0 + tx;
+        if (u <= n && z < zs) Y[((long)(y + n / 2) * (n + 1) + u) * zs + z] = tile[tx][j];
+    }
+}
+
+// RT stage: B[n/2 + y][u][z] -> X[z][y][u], halving the interior columns
+// (transpose of the R2C along x: the C2R counts them twice).
+__global__ void k_transpose_out(const float2* __restrict__ B, float2* __restrict__ X, int n, int zs) {
+    __shared__ float2 tile[32][33];
+    const int u0 = blockIdx.x * 32, z0 = blockIdx.y * 32, y = blockIdx.z;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int j = ty; j < 32; j += 8) {
+        const int u = u0 + j, z = z0 + tx;
+        if (u <= n && z < zs) tile[j][tx] = __ldg(B + ((long)(y + n / 2) * (n + 1) + u) * zs + z);
+    }
+    __syncthreads();
+    for (int j = ty; j < 32; j += 8) {
+        const int z = z0 + j, u = u0 + tx;
+        if (z < zs && u <= n) {
+            float2 v = tile[tx][j];
+            // the C2R reads only the real part of its DC and Nyquist bins; cuFFT
+            // leaves the imaginary part's effect undefined, so clear it here
+            if (u > 0 && u < n) { v.x *= 0.5f; v.y *= 0.5f; } else { v.y = 0.f; }
+            X[((long)z * n + y) * (n + 1) + u] = v;
+        }
+    }
+}
+
+// R stage 5: Gaussian gather of the n/2+1 non-redundant samples per angle.
+// One group of LPS lanes per sample; each lane owns ZV slices.
+template <int ZV, int LPS, int M>
+__global__ void __launch_bounds__(kThreads) k_gather(const float2* __restrict__ F, float2* __restrict__ H,
+                                                     const float* __restrict__ cosT, const float* __restrict__ sinT,
+                                                     int n, int T, int zs, float c0, float c1, float scale,
+                                                     int clamp) {
+    constexpr int L = 2 * M + 1;
+    constexpr int SPW = 32 / LPS;
+    const int K = n / 2 + 1;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / LPS, zl = lane % LPS;
+    const int zgroups = zs / (LPS * ZV);
+    const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long zg = warp % zgroups;
+    const long s = (warp / zgroups) * SPW + sub;
+    if (s >= (long)T * K) return;
+    const int t = (int)(s / K), k = (int)(s % K);
+    const SampleGeo g = sample_geo(t, k, n, M, cosT, sinT, clamp != 0);
+    const float inv_twon = 1.0f / (float)(2 * n);
+    float wx[L], wy[L];
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+        wx[i] = tap_weight(g.bx + i, g.x0, inv_twon, c1);
+        wy[i] = c0 * tap_weight(g.by + i, g.y0, inv_twon, c1);
+    }
+    const int zoff = (int)zg * (LPS * ZV) + zl * ZV;
+    const long rowstride = (long)(n + 1) * zs;
+    const int twon = 2 * n;
+    float acc[2 * ZV];
+#pragma unroll
+    for (int q = 0; q < 2 * ZV; ++q) acc[q] = 0.f;
+    const bool fast = (g.bx >= 0) && (g.bx + 2 * M <= n);
+#pragma unroll
+    for (int i1 = 0; i1 < L; ++i1) {
+        float ar[2 * ZV];
+#pragma unroll
+        for (int q = 0; q < 2 * ZV; ++q) ar[q] = 0.f;
+        const int v = g.by + i1;
+        if (fast) {
+            const int row = v < 0 ? v + twon : (v >= twon ? v - twon : v);
+            const float2* p = F + row * rowstride + (long)g.bx * zs + zoff;
+#pragma unroll
+            for (int i0 = 0; i0 < L; ++i0) {
+                float val[2 * ZV];
+                ZVec<ZV>::load(p + (long)i0 * zs, val);
+#pragma unroll
+                for (int q = 0; q < 2 * ZV; ++q) ar[q] = fmaf(wx[i0], val[q], ar[q]);
+            }
+        } else {
+#pragma unroll
+            for (int i0 = 0; i0 < L; ++i0) {
+                int row, col;
+                bool cj;
+                tap_cell(g.bx + i0, v, n, row, col, cj);
+                float val[2 * ZV];
+                ZVec<ZV>::load(F + row * rowstride + (long)col * zs + zoff, val);
+                if (cj) {
+#pragma unroll
+                    for (int q = 1; q < 2 * ZV; q += 2) val[q] = -val[q];
+                }
+#pragma unroll
+                for (int q = 0; q < 2 * ZV; ++q) ar[q] = fmaf(wx[i0], val[q], ar[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 2 * ZV; ++q) acc[q] = fmaf(wy[i1], ar[q], acc[q]);
+    }
+    const float sc = (g.j & 1) ? -scale : scale;
+    // k = 0 and k = n/2 are the DC and Nyquist bins of the C2R along r: only
+    // their real part enters the result (the .real of tomo.py:150)
+    const float si = (k == 0 || k == n / 2) ? 0.f : (g.mir ? -sc : sc);
+#pragma unroll
+    for (int q = 0; q < 2 * ZV; q += 2) {
+        acc[q] *= sc;
+        acc[q + 1] *= si;
+    }
+    ZVec<ZV>::store(H + ((long)k * T + t) * zs + zoff, acc);
+}
+
+// RT: pull-scatter over the static CSR table.  One lane group per cell.
+template <int ZV, int LPS>
+__global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict__ ptr,
+                                                      const unsigned* __restrict__ idx,
+                                                      const float* __restrict__ wgt,
+                                                      const float2* __restrict__ Q, float2* __restrict__ A,
+                                                      long ncells, int zs) {
+    constexpr int SPW = 32 / LPS;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / LPS, zl = lane % LPS;
+    const int zgroups = zs / (LPS * ZV);
+    const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long zg = warp % zgroups;
+    const long c = (warp / zgroups) * SPW + sub;
+    if (c >= ncells) return;
+    const int zoff = (int)zg * (LPS * ZV) + zl * ZV;
+    float acc[2 * ZV];
+#pragma unroll
+    for (int q = 0; q < 2 * ZV; ++q) acc[q] = 0.f;
+    const unsigned e0 = __ldg(ptr + c), e1 = __ldg(ptr + c + 1);
+    unsigned e = e0;
+    for (; e + 2 <= e1; e += 2) {
+        const unsigned ia = __ldg(idx + e), ib = __ldg(idx + e + 1);
+        const float wa = __ldg(wgt + e), wb = __ldg(wgt + e + 1);
+        float va[2 * ZV], vb[2 * ZV];
+        ZVec<ZV>::load(Q + (long)(ia & 0x7fffffffu) * zs + zoff, va);
+        ZVec<ZV>::load(Q + (long)(ib & 0x7fffffffu) * zs + zoff, vb);
+        const float sa = (ia >> 31) ? -wa : wa, sb = (ib >> 31) ? -wb : wb;
+#pragma unroll
+        for (int q = 0; q < 2 * ZV; q += 2) {
+            acc[q] = fmaf(wa, va[q], acc[q]);
+            acc[q + 1] = fmaf(sa, va[q + 1], acc[q + 1]);
+        }
+#pragma unroll
+        for (int q = 0; q < 2 * ZV; q += 2) {
+            acc[q] = fmaf(wb, vb[q], acc[q]);
+            acc[q + 1] = fmaf(sb, vb[q + 1], acc[q + 1]);
+        }
+    }
+    if (e < e1) {
+        const unsigned ia = __ldg(idx + e);
+        const float wa = __ldg(wgt + e);
+        float va[2 * ZV];
+        ZVec<ZV>::load(Q + (long)(ia & 0x7fffffffu) * zs + zoff, va);
+        const float sa = (ia >> 31) ? -wa : wa;
+#pragma unroll
+        for (int q = 0; q < 2 * ZV; q += 2) {
+            acc[q] = fmaf(wa, va[q], acc[q]);
+            acc[q + 1] = fmaf(sa, va[q + 1], acc[q + 1]);
+        }
+    }
+    ZVec<ZV>::store(A + c * zs + zoff, acc);
+}
+
+// Scatter-table construction ---------------------------------------------
+// Key of entry e = (sample s, tap): (cell << 32) | e, with e = s*L*L + tap.
+template <int M>
+__global__ void k_csr_keys(unsigned long long* __restrict__ keys, const float* __restrict__ cosT,
+                           const float* __restrict__ sinT, int n, int T, long nent) {
+    constexpr int L = 2 * M + 1;
+    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nent) return;
+    const int K = n / 2 + 1;
+    const long s = e / (L * L);
+    const int tap = (int)(e % (L * L));
+    const int t = (int)(s / K), k = (int)(s % K);
+    const SampleGeo g = sample_geo(t, k, n, M, cosT, sinT);
+    int row, col;
+    bool cj;
+    tap_cell(g.bx + tap % L, g.by + tap / L, n, row, col, cj);
+    const unsigned long long cell = (unsigned long long)row * (n + 1) + col;
+    keys[e] = (cell << 32) | (unsigned long long)e;
+}
+
+template <int M>
+__global__ void k_csr_payload(const unsigned long long* __restrict__ keys, unsigned* __restrict__ idx,
+                              float* __restrict__ wgt, const float* __restrict__ cosT,
+                              const float* __restrict__ sinT, int n, int T, long nent, float c0, float c1,
+                              float scale) {
+    constexpr int L = 2 * M + 1;
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nent) return;
+    const long e = (long)(keys[i] & 0xffffffffull);
+    const int K = n / 2 + 1;
+    const long s = e / (L * L);
+    const int tap = (int)(e % (L * L));
+    const int t = (int)(s / K), k = (int)(s % K);
+    const SampleGeo g = sample_geo(t, k, n, M, cosT, sinT);
+    const int i0 = tap % L, i1 = tap / L;
+    const float inv_twon = 1.0f / (float)(2 * n);
+    const float wx = tap_weight(g.bx + i0, g.x0, inv_twon, c1);
+    const float wy = c0 * tap_weight(g.by + i1, g.y0, inv_twon, c1);
+    int row, col;
+    bool cj;
+    tap_cell(g.bx + i0, g.by + i1, n, row, col, cj);
+    // transpose of H = (-1)^j g / (4n^2) followed by the C2R along r, which
+    // counts the interior bins twice
+    const float ck = (k > 0 && k < n / 2) ? 2.f : 1.f;
+    const float sj = (g.j & 1) ? -1.f : 1.f;
+    wgt[i] = (wy * wx) * (ck * sj * scale);
+    idx[i] = (unsigned)((long)k * T + t) | ((cj != g.mir) ? 0x80000000u : 0u);
+}
+
+__global__ void k_csr_ptr(const unsigned long long* __restrict__ keys, unsigned* __restrict__ ptr, long nent,
+                          long ncells) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > nent) return;
+    const long prev = (i == 0) ? -1 : (long)(keys[i - 1] >> 32);
+    const long cur = (i == nent) ? ncells : (long)(keys[i] >> 32);
+    for (long c = prev + 1; c <= cur; ++c) ptr[c] = (unsigned)i;
+}
+
+// RT final stage: obj = phi * crop(Q); OUT = 0 real, 1/2 real/imag part of c64.
+template <int OUT>
+__global__ void k_crop_phi(const float* __restrict__ Q, void* __restrict__ obj, const float* __restrict__ phi1,
+                           float phis, int n) {
+    const long row = blockIdx.x;  // z * n + y
+    const int y = (int)(row % n);
+    const float py = phis * __ldg(phi1 + y);
+    const float* src = Q + row * 2 * n + n / 2;
+    for (int x = threadIdx.x; x < n; x += blockDim.x) {
+        const float v = py * __ldg(phi1 + x) * __ldg(src + x);
+        if (OUT == 0)
+            static_cast<float*>(obj)[row * n + x] = v;
+        else
+            static_cast<float*>(obj)[(row * n + x) * 2 + (OUT - 1)] = v;
+    }
+}
+
+// (T, zs, n) -> (T, nzc, n) and back, zero-filling the extra slices.
+__global__ void k_copy_z(const float* __restrict__ src, float* __restrict__ dst, int n, int zsrc, int zdst,
+                         int zvalid) {
+    const long row = blockIdx.x;  // t * zdst + z
+    const int z = (int)(row % zdst);
+    const long t = row / zdst;
+    float* d = dst + row * n;
+    const float* s = src + (t * zsrc + z) * n;
+    for (int x = threadIdx.x; x < n; x += blockDim.x) d[x] = (z < zvalid) ? __ldg(s + x) : 0.f;
+}
+__global__ void k_copy_z_c(const float2* __restrict__ src, float2* __restrict__ dst, int n, int zsrc, int zdst,
+                           int zvalid) {
+    const long row = blockIdx.x;
+    const int z = (int)(row % zdst);
+    const long t = row / zdst;
+    float2* d = dst + row * n;
+    const float2* s = src + (t * zsrc + z) * n;
+    for (int x = threadIdx.x; x < n; x += blockDim.x) d[x] = (z < zvalid) ? __ldg(s + x) : make_float2(0.f, 0.f);
+}
+
+// Complex RT: Hermitian (PART=0) or anti-Hermitian times -i (PART=1) part of
+// the line spectra, in the scatter's input layout Q[k][t][z].
+template <int PART>
+__global__ void k_combine(const float2* __restrict__ Yc, float2* __restrict__ Q, int n, int T, int zs) {
+    const long row = blockIdx.x;  // t * zs + z
+    const int z = (int)(row % zs);
+    const long t = row / zs;
+    const float2* y = Yc + row * n;
+    const int K = n / 2 + 1;
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const float2 a = __ldg(y + k);
+        float2 q;
+        if (k == 0 || k == n / 2) {
+            q = a;
+        } else {
+            const float2 b = __ldg(y + (n - k));
+            q = PART == 0 ? make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y))
+                          : make_float2(0.5f * (a.x - b.x), 0.5f * (a.y + b.y));
+        }
+        if (PART == 1) q = make_float2(q.y, -q.x);  // times -i
+        Q[((long)k * T + t) * zs + z] = q;
+    }
+}
+
+// --------------------------------------------------------------------------
+int plan1d(cufftHandle* plan, long long len, long long istride, long long idist, long long ostride,
+           long long odist, cufftType type, long long batch, size_t* work) {
+    MM_CUFFT(cufftCreate(plan));
+    MM_CUFFT(cufftSetAutoAllocation(*plan, 0));
+    long long nn[1] = {len};
+    const bool r2c = type == CUFFT_R2C, c2r = type == CUFFT_C2R;
+    long long inemb[1] = {c2r ? len / 2 + 1 : len};
+    long long onemb[1] = {r2c ? len / 2 + 1 : len};
+    size_t ws = 0;
+    MM_CUFFT(cufftMakePlanMany64(*plan, 1, nn, inemb, istride, idist, onemb, ostride, odist, type, batch, &ws));
+    *work = std::max(*work, ws);
+    return MM_OK;
+}
+
+// One work area shared by every cuFFT plan of the handle (they run in
+// sequence on one stream); grown when a new plan needs more, and attached to
+// every plan each time a plan is added.
+int ensure_work(mm_tomo* h, size_t need) {
+    if (need > h->fft_work_bytes || !h->fft_work) {
+        if (h->fft_work) {
+            cudaFree(h->fft_work);
+            h->ws_bytes -= h->fft_work_bytes;
+            h->fft_work = nullptr;
+            h->fft_work_bytes = 0;
+        }
+        MM_TRY(dev_alloc(&h->fft_work, need, "cuFFT work area"));
+        h->fft_work_bytes = need;
+        h->ws_bytes += need;
+    }
+    cufftHandle all[6] = {h->plan_xr2c, h->plan_xc2r, h->plan_y, h->plan_rc2r, h->plan_rr2c, h->plan_rc2c};
+    for (cufftHandle p : all)
+        if (p) MM_CUFFT(cufftSetWorkArea(p, h->fft_work));
+    return MM_OK;
+}
+
+template <typename Tp>
+int alloc(mm_tomo* h, Tp** p, size_t count, const char* what) {
+    void* q = nullptr;
+    MM_TRY(dev_alloc(&q, count * sizeof(Tp), what));
+    *p = static_cast<Tp*>(q);
+    h->ws_bytes += count * sizeof(Tp);
+    return MM_OK;
+}
+
+int pick_lanes(int zs, int& ZV, int& LPS) {
+    if (zs >= 64) { ZV = 2; LPS = 32; }
+    else { ZV = 1; LPS = zs; }
+    return MM_OK;
+}
+
+template <int ZV, int LPS>
+int launch_gather_m(mm_tomo* h, cudaStream_t st) {
+    const int K = h->K;
+    const long samples = (long)h->ntheta * K;
+    const long warps = ((samples + (32 / LPS) - 1) / (32 / LPS)) * (h->zs / (LPS * ZV));
+    const long blocks = (warps * 32 + kThreads - 1) / kThreads;
+    const float scale = (float)(1.0 / (4.0 * h->n * (double)h->n));
+#define MM_G(MM)                                                                                 \
+    case MM:                                                                                     \
+        k_gather<ZV, LPS, MM><<<blocks, kThreads, 0, st>>>(h->F, h->Hh, h->d_cos, h->d_sin, h->n, \
+                                                           h->ntheta, h->zs, h->c0, h->c1, scale, \
+                                                           h->clamp);                              \
+        break;
+    switch (h->m) {
+        MM_G(2) MM_G(3) MM_G(4) MM_G(5) MM_G(6)
+        default: MM_REQUIRE(false, "unsupported m=%d", h->m);
+    }
+#undef MM_G
+    MM_LAUNCHED();
+    return MM_OK;
+}
+
+int launch_gather(mm_tomo* h, cudaStream_t st) {
+    int ZV, LPS;
+    pick_lanes(h->zs, ZV, LPS);
+    if (ZV == 2) return launch_gather_m<2, 32>(h, st);
+    switch (LPS) {
+        case 1: return launch_gather_m<1, 1>(h, st);
+        case 2: return launch_gather_m<1, 2>(h, st);
+        case 4: return launch_gather_m<1, 4>(h, st);
+        case 8: return launch_gather_m<1, 8>(h, st);
+        case 16: return launch_gather_m<1, 16>(h, st);
+        default: return launch_gather_m<1, 32>(h, st);
+    }
+}
+
+template <int ZV, int LPS>
+int launch_scatter_t(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) {
+    const long ncells = 2L * h->n * (h->n + 1);
+    const long warps = ((ncells + (32 / LPS) - 1) / (32 / LPS)) * (h->zs / (LPS * ZV));
+    const long blocks = (warps * 32 + kThreads - 1) / kThreads;
+    k_scatter<ZV, LPS><<<blocks, kThreads, 0, st>>>(h->csr_ptr, h->csr_idx, h->csr_w, Q, A, ncells, h->zs);
+    MM_LAUNCHED();
+    return MM_OK;
+}
+
+int launch_scatter(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) {
+    int ZV, LPS;
+    pick_lanes(h->zs, ZV, LPS);
+    if (ZV == 2) return launch_scatter_t<2, 32>(h, Q, A, st);
+    switch (LPS) {
+        case 1: return launch_scatter_t<1, 1>(h, Q, A, st);
+        case 2: return launch_scatter_t<1, 2>(h, Q, A, st);
+        case 4: return launch_scatter_t<1, 4>(h, Q, A, st);
+        case 8: return launch_scatter_t<1, 8>(h, Q, A, st);
+        case 16: return launch_scatter_t<1, 16>(h, Q, A, st);
+        default: return launch_scatter_t<1, 32>(h, Q, A, st);
+    }
+}
+
+int build_csr(mm_tomo* h, cudaStream_t st) {
+    if (h->csr_ready) return MM_OK;
+    const int n = h->n, T = h->ntheta, M = h->m, L = 2 * M + 1;
+    const long nent = (long)T * h->K * L * L;
+    const long ncells = 2L * n * (n + 1);
+    MM_REQUIRE(nent < (1L << 32) && (long)T * h->K < (1L << 31), "adjoint table too large: %ld entries", nent);
+    int cellbits = 1;
+    while ((1L << cellbits) < ncells) ++cellbits;
+    unsigned long long *kin = nullptr, *kout = nullptr;
+    void* tmp = nullptr;
+    size_t tmp_bytes = 0;
+    int rc = MM_OK;
+    auto cleanup = [&]() {
+        if (kin) cudaFree(kin);
+        if (kout) cudaFree(kout);
+        if (tmp) cudaFree(tmp);
+    };
+    if ((rc = dev_alloc((void**)&kin, nent * 8, "scatter keys")) != MM_OK) return cleanup(), rc;
+    if ((rc = dev_alloc((void**)&kout, nent * 8, "scatter keys (sorted)")) != MM_OK) return cleanup(), rc;
+    cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, kin, kout, (int64_t)nent, 0, 32 + cellbits, st);
+    if ((rc = dev_alloc(&tmp, tmp_bytes, "radix sort temp")) != MM_OK) return cleanup(), rc;
+    if ((rc = alloc(h, &h->csr_ptr, ncells + 1, "scatter row pointers")) != MM_OK) return cleanup(), rc;
+    if ((rc = alloc(h, &h->csr_idx, nent, "scatter sample index")) != MM_OK) return cleanup(), rc;
+    if ((rc = alloc(h, &h->csr_w, nent, "scatter weights")) != MM_OK) return cleanup(), rc;
+    const long gb = (nent + kThreads - 1) / kThreads;
+    const float scale = (float)(1.0 / (4.0 * n * (double)n));
+#define MM_K(MM)                                                                                        \
+    case MM:                                                                                            \
+        k_csr_keys<MM><<<gb, kThreads, 0, st>>>(kin, h->d_cos, h->d_sin, n, T, nent);                   \
+        break;
+    switch (M) {
+        MM_K(2) MM_K(3) MM_K(4) MM_K(5) MM_K(6)
+        default: cleanup(); MM_REQUIRE(false, "unsupported m=%d", M);
+    }
+#undef MM_K
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, kin, kout, (int64_t)nent, 0, 32 + cellbits, st);
+    if (e == cudaSuccess) {
+#define MM_P(MM)                                                                                          \
+    case MM:                                                                                              \
+        k_csr_payload<MM><<<gb, kThreads, 0, st>>>(kout, h->csr_idx, h->csr_w, h->d_cos, h->d_sin, n, T, \
+                                                   nent, h->c0, h->c1, scale);                            \
+        break;
+        switch (M) { MM_P(2) MM_P(3) MM_P(4) MM_P(5) MM_P(6) }
+#undef MM_P
+        k_csr_ptr<<<(nent + 1 + kThreads - 1) / kThreads, kThreads, 0, st>>>(kout, h->csr_ptr, nent, ncells);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cleanup();
+    if (e != cudaSuccess) {
+        mm::set_error("building the adjoint scatter table: %s", cudaGetErrorString(e));
+        return MM_ECUDA;
+    }
+    h->nnz = nent;
+    h->csr_ready = true;
+    return MM_OK;
+}
+
+int ensure_rt(mm_tomo* h, cudaStream_t st) {
+    if (!h->plans_rt) {
+        const int n = h->n, T = h->ntheta, zs = h->zs;
+        size_t ws = h->fft_work_bytes;
+        MM_TRY(plan1d(&h->plan_rr2c, n, 1, n, (long long)T * zs, 1, CUFFT_R2C, (long long)T * zs, &ws));
+        MM_TRY(plan1d(&h->plan_xc2r, 2 * n, 1, n + 1, 1, 2 * n, CUFFT_C2R, (long long)zs * n, &ws));
+        h->plans_rt = true;
+        MM_TRY(ensure_work(h, ws));
+    }
+    return build_csr(h, st);
+}
+
+void destroy(mm_tomo* h) {
+    cufftHandle all[6] = {h->plan_xr2c, h->plan_xc2r, h->plan_y, h->plan_rc2r, h->plan_rr2c, h->plan_rc2c};
+    for (cufftHandle p : all)
+        if (p) cufftDestroy(p);
+    void* bufs[] = {h->d_cos, h->d_sin, h->d_phi1, h->P, h->X, h->Y, h->F, h->Hh, h->sino_tmp, h->fft_work,
+                    h->csr_ptr, h->csr_idx, h->csr_w, h->ypad, h->yc};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    delete h;
+}
+
+}  // namespace
+
+// ==========================================================================
+extern "C" int mm_tomo_create(int n, int nz, int ntheta, const float* theta_host, const mm_tomo_opts* opts,
+                              mm_tomo** out) {
+    MM_REQUIRE(out != nullptr, "mm_tomo_create: out is NULL");
+    *out = nullptr;
+    MM_REQUIRE(n >= 8 && n <= 16384 && n % 2 == 0, "mm_tomo_create: n=%d must be even and in [8, 16384]", n);
+    MM_REQUIRE(nz >= 1 && nz <= 4096, "mm_tomo_create: nz=%d out of range", nz);
+    MM_REQUIRE(ntheta >= 1 && theta_host != nullptr, "mm_tomo_create: need ntheta >= 1 angles");
+    const double eps = (opts && opts->eps > 0) ? opts->eps : 1e-3;
+    const double mu = -log(eps) / (2.0 * n * n);
+    int m = (int)ceil(2.0 * n / M_PI * sqrt(-mu * log(eps) + (mu * n) * (mu * n) / 4.0));
+    if (opts && opts->m > 0) m = opts->m;
+    MM_REQUIRE(m >= 2 && m <= 6, "mm_tomo_create: m=%d unsupported (2..6)", m);
+
+    mm_tomo* h = new mm_tomo();
+    h->n = n;
+    h->nz = nz;
+    h->ntheta = ntheta;
+    h->m = m;
+    h->K = n / 2 + 1;
+    h->clamp = (opts && opts->clamp_xy) ? 1 : 0;
+    int zs = 1;
+    while (zs < nz) zs <<= 1;
+    h->zs = zs;
+    h->mu = (float)mu;  // the reference hands mu to its kernels as float32
+    h->c0 = 3.141592653589793238f / h->mu;
+    h->c1 = -3.141592653589793238f * 3.141592653589793238f / h->mu;
+    h->phi_scale = (float)((double)(1 - n % 4) / (n * sqrt((double)n * ntheta)));
+    cudaGetDevice(&h->device);
+
+    auto fail = [&](int rc) {
+        destroy(h);
+        return rc;
+    };
+    int rc;
+    std::vector<float> cs(ntheta), sn(ntheta), ph(n);
+    for (int t = 0; t < ntheta; ++t) {
+        cs[t] = (float)cos((double)theta_host[t]);
+        sn[t] = (float)sin((double)theta_host[t]);
+    }
+    for (int i = 0; i < n; ++i) {
+        const float tf = (float)(-0.5 + (double)i / n);   // linspace(-1/2, 1/2, n) in float32
+        const double td = tf;
+        ph[i] = (float)exp(mu * (double)n * n * td * td);
+    }
+    if ((rc = alloc(h, &h->d_cos, ntheta, "cos table")) || (rc = alloc(h, &h->d_sin, ntheta, "sin table")) ||
+        (rc = alloc(h, &h->d_phi1, n, "phi table")))
+        return fail(rc);
+    if (cudaMemcpy(h->d_cos, cs.data(), ntheta * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(h->d_sin, sn.data(), ntheta * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(h->d_phi1, ph.data(), n * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+        mm::set_error("mm_tomo_create: table upload failed");
+        return fail(MM_ECUDA);
+    }
+    const size_t spec = (size_t)2 * n * (n + 1) * zs;
+    if ((rc = alloc(h, &h->P, (size_t)zs * n * 2 * n, "padded rows")) ||
+        (rc = alloc(h, &h->X, (size_t)zs * n * (n + 1), "row spectra")) ||
+        (rc = alloc(h, &h->Y, spec, "padded column input")) || (rc = alloc(h, &h->F, spec, "half spectrum")) ||
+        (rc = alloc(h, &h->Hh, (size_t)h->K * ntheta * zs, "polar lines")))
+        return fail(rc);
+    if (cudaMemset(h->Y, 0, spec * sizeof(float2)) != cudaSuccess) {
+        mm::set_error("mm_tomo_create: memset failed");
+        return fail(MM_ECUDA);
+    }
+    size_t ws = 0;
+    if ((rc = plan1d(&h->plan_xr2c, 2 * n, 1, 2 * n, 1, n + 1, CUFFT_R2C, (long long)zs * n, &ws)) ||
+        (rc = plan1d(&h->plan_y, 2 * n, (long long)(n + 1) * zs, 1, (long long)(n + 1) * zs, 1, CUFFT_C2C,
+                     (long long)(n + 1) * zs, &ws)) ||
+        (rc = plan1d(&h->plan_rc2r, n, (long long)ntheta * zs, 1, 1, n, CUFFT_C2R, (long long)ntheta * zs, &ws)) ||
+        (rc = ensure_work(h, ws)))
+        return fail(rc);
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        mm::set_error("mm_tomo_create: device error during setup");
+        return fail(MM_ECUDA);
+    }
+    *out = h;
+    return MM_OK;
+}
+
+extern "C" int mm_tomo_destroy(mm_tomo* h) {
+    if (!h) return MM_OK;
+    cudaDeviceSynchronize();
+    destroy(h);
+    return MM_OK;
+}
+
+extern "C" size_t mm_tomo_workspace_bytes(const mm_tomo* h) { return h ? h->ws_bytes : 0; }
+
+extern "C" int mm_tomo_R(mm_tomo* h, const float* obj, float* sino, int nz, void* stream) {
+    MM_REQUIRE(h != nullptr, "mm_tomo_R: NULL handle");
+    MM_REQUIRE(obj != nullptr && sino != nullptr, "mm_tomo_R: NULL array");
+    MM_REQUIRE(nz >= 1 && nz <= h->nz, "mm_tomo_R: nz=%d outside [1, %d]", nz, h->nz);
+    MM_REQUIRE(((uintptr_t)obj % 4) == 0 && ((uintptr_t)sino % 4) == 0, "mm_tomo_R: misaligned array");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int n = h->n, zs = h->zs, T = h->ntheta;
+    if (h->y_dirty) {  // rows [0, n/2) and [3n/2, 2n) of Y are the y zero padding
+        const size_t half = (size_t)(n / 2) * (n + 1) * zs * sizeof(float2);
+        MM_CUDA(cudaMemsetAsync(h->Y, 0, half, st));
+        MM_CUDA(cudaMemsetAsync(h->Y + (size_t)(3 * n / 2) * (n + 1) * zs, 0, half, st));
+        h->y_dirty = false;
+    }
+    k_pad_phi<<<(unsigned)((long)zs * n), kThreads, 0, st>>>(obj, h->P, h->d_phi1, h->phi_scale, n, nz);
+    MM_LAUNCHED();
+    MM_CUFFT(cufftSetStream(h->plan_xr2c, st));
+    MM_CUFFT(cufftExecR2C(h->plan_xr2c, h->P, (cufftComplex*)h->X));
+    dim3 tb(32, 8), tg((n + 1 + 31) / 32, (zs + 31) / 32, n);
+    k_transpose_in<<<tg, tb, 0, st>>>(h->X, h->Y, n, zs);
+    MM_LAUNCHED();
+    MM_CUFFT(cufftSetStream(h->plan_y, st));
+    MM_CUFFT(cufftExecC2C(h->plan_y, (cufftComplex*)h->Y, (cufftComplex*)h->F, CUFFT_FORWARD));
+    MM_TRY(launch_gather(h, st));
+    float* dst = sino;
+    if (nz < zs) {
+        if (!h->sino_tmp) MM_TRY(alloc(h, &h->sino_tmp, (size_t)T * zs * n, "padded sinogram"));
+        dst = h->sino_tmp;
+    }
+    MM_CUFFT(cufftSetStream(h->plan_rc2r, st));
+    MM_CUFFT(cufftExecC2R(h->plan_rc2r, (cufftComplex*)h->Hh, dst));
+    if (nz < zs) {
+        k_copy_z<<<(unsigned)((long)T * nz), kThreads, 0, st>>>(h->sino_tmp, sino, n, zs, nz, nz);
+        MM_LAUNCHED();
+    }
+    return MM_OK;
+}
+
+extern "C" int mm_tomo_prepare_rt(mm_tomo* h, void* stream) {
+    MM_REQUIRE(h != nullptr, "mm_tomo_prepare_rt: NULL handle");
+    return ensure_rt(h, (cudaStream_t)stream);
+}
+
+namespace {
+// scatter + IFFT along v + transposed C2R along x + crop*phi for one real
+// run whose line spectra are in Q = h->Hh.  OUT selects the output part.
+int rt_tail(mm_tomo* h, void* obj, int out, cudaStream_t st) {
+    const int n = h->n, zs = h->zs;
+    MM_TRY(launch_scatter(h, h->Hh, h->F, st));
+    MM_CUFFT(cufftSetStream(h->plan_y, st));
+    MM_CUFFT(cufftExecC2C(h->plan_y, (cufftComplex*)h->F, (cufftComplex*)h->Y, CUFFT_INVERSE));
+    h->y_dirty = true;
+    dim3 tb(32, 8), tg((n + 1 + 31) / 32, (zs + 31) / 32, n);
+    k_transpose_out<<<tg, tb, 0, st>>>(h->Y, h->X, n, zs);
+    MM_LAUNCHED();
+    MM_CUFFT(cufftSetStream(h->plan_xc2r, st));
+    MM_CUFFT(cufftExecC2R(h->plan_xc2r, (cufftComplex*)h->X, h->P));
+    return MM_OK;
+}
+}  // namespace
+
+extern "C" int mm_tomo_RT(mm_tomo* h, const void* sino, int dtype, void* obj, int nz, void* stream) {
+    MM_REQUIRE(h != nullptr, "mm_tomo_RT: NULL handle");
+    MM_REQUIRE(sino != nullptr && obj != nullptr, "mm_tomo_RT: NULL array");
+    MM_REQUIRE(dtype == MM_F32 || dtype == MM_C64, "mm_tomo_RT: dtype %d unsupported", dtype);
+    MM_REQUIRE(nz >= 1 && nz <= h->nz, "mm_tomo_RT: nz=%d outside [1, %d]", nz, h->nz);
+    MM_REQUIRE(((uintptr_t)sino % (dtype == MM_C64 ? 8 : 4)) == 0 && ((uintptr_t)obj % 4) == 0,
+               "mm_tomo_RT: misaligned array");
+    cudaStream_t st = (cudaStream_t)stream;
+    MM_TRY(ensure_rt(h, st));
+    const int n = h->n, zs = h->zs, T = h->ntheta;
+    const unsigned rows = (unsigned)((long)nz * n);
+    if (dtype == MM_F32) {
+        const float* y = static_cast<const float*>(sino);
+        if (nz < zs) {
+            if (!h->ypad) MM_TRY(alloc(h, &h->ypad, (size_t)T * zs * n, "padded sinogram"));
+            k_copy_z<<<(unsigned)((long)T * zs), kThreads, 0, st>>>(y, h->ypad, n, nz, zs, nz);
+            MM_LAUNCHED();
+            y = h->ypad;
+        }
+        MM_CUFFT(cufftSetStream(h->plan_rr2c, st));
+        MM_CUFFT(cufftExecR2C(h->plan_rr2c, (cufftReal*)y, (cufftComplex*)h->Hh));
+        MM_TRY(rt_tail(h, obj, 0, st));
+        k_crop_phi<0><<<rows, kThreads, 0, st>>>(h->P, obj, h->d_phi1, h->phi_scale, n);
+        MM_LAUNCHED();
+        return MM_OK;
+    }
+    // complex64 sinogram: real and imaginary output parts are two real runs
+    if (!h->plans_c) {
+        size_t ws = h->fft_work_bytes;
+        MM_TRY(plan1d(&h->plan_rc2c, n, 1, n, 1, n, CUFFT_C2C, (long long)T * zs, &ws));
+        h->plans_c = true;
+        MM_TRY(ensure_work(h, ws));
+    }
+    if (!h->yc) MM_TRY(alloc(h, &h->yc, (size_t)T * zs * n, "complex line spectra"));
+    const float2* y = static_cast<const float2*>(sino);
+    if (nz < zs) {
+        k_copy_z_c<<<(unsigned)((long)T * zs), kThreads, 0, st>>>(y, h->yc, n, nz, zs, nz);
+        MM_LAUNCHED();
+        y = h->yc;
+    }
+    MM_CUFFT(cufftSetStream(h->plan_rc2c, st));
+    MM_CUFFT(cufftExecC2C(h->plan_rc2c, (cufftComplex*)y, (cufftComplex*)h->yc, CUFFT_FORWARD));
+    for (int part = 0; part < 2; ++part) {
+        if (part == 0)
+            k_combine<0><<<(unsigned)((long)T * zs), kThreads, 0, st>>>(h->yc, h->Hh, n, T, zs);
+        else
+            k_combine<1><<<(unsigned)((long)T * zs), kThreads, 0, st>>>(h->yc, h->Hh, n, T, zs);
+        MM_LAUNCHED();
+        MM_TRY(rt_tail(h, obj, part + 1, st));
+        if (part == 0)
+            k_crop_phi<1><<<rows, kThreads, 0, st>>>(h->P, obj, h->d_phi1, h->phi_scale, n);
+        else
+            k_crop_phi<2><<<rows, kThreads, 0, st>>>(h->P, obj, h->d_phi1, h->phi_scale, n);
+        MM_LAUNCHED();
+    }
+    return MM_OK;
+}
