@@ -1,0 +1,403 @@
+"""Benchmark of the forward-model hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload production|small]
+
+One step of the default ("production") workload is the hot path of the
+pipeline at 64 slices of 2048^2: the USFFT Radon transform R of the volume
+at 2058 angles on [0, 2 pi), then psi = exp(-p s/beta_r)(cos p s, sin p s),
+Fresnel propagation D (30 keV, 0.12 m, 0.69 um pixels, 2x mirror padding)
+and |.|^2 of all 2058 projections.  The metric is R/RT throughput in
+Gvox*angle/s = slices * n^2 * ntheta / step time (whole job, all ranks); the
+adjoint RT is timed on the same data and reported beside it.
+
+Rank layout: one process per GPU (torchrun for N > 1); every rank runs its
+own 64-slice slab (weak scaling, no collective on the data path; the ranks
+only meet at barriers and in a max-reduce of their timings).
+
+--impl reference times the reference's own kernels (processing/kernels.py,
+compiled for the host into oracle/_ref by oracle/build_ref.py) with the
+reference's host glue restated in NumPy/SciPy on all host cores, on a bounded
+sample of the same workload (one slice of R plus 32 frames of D, scaled to a
+full step).  Under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # 64 slices of 2048^2, 2058 angles on [0, 2 pi), then D of all projections
+    "production": dict(n=2048, nz=64, ntheta=2058, theta_max=2 * np.pi, energy_kev=30.0,
+                       distance=0.12, voxelsize=0.69e-6),
+    # 128 slices of 128^2, 180 angles on [0, pi)
+    "small": dict(n=128, nz=128, ntheta=180, theta_max=np.pi, energy_kev=30.0,
+                  distance=0.12, voxelsize=0.69e-6),
+    # same kernels as "production" on a few GB of device memory (for ncu captures)
+    "profile": dict(n=1024, nz=64, ntheta=512, theta_max=2 * np.pi, energy_kev=30.0,
+                    distance=0.12, voxelsize=0.69e-6),
+}
+BETA_RATIO = 100.0
+L2_BYTES = 126 * 2 ** 20
+
+
+def workload_desc(w, name):
+    return (f"{name}: R of {w['nz']} slices of {w['n']}^2 at {w['ntheta']} angles on "
+            f"[0, {'2pi' if w['theta_max'] > 4 else 'pi'}), then psi -> Fresnel D ({w['energy_kev']:g} keV, "
+            f"{w['distance']} m, {w['voxelsize'] * 1e6:.2f} um, 2x mirror pad) -> |.|^2 of all projections")
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(kernel):
+    """Per-launch DRAM bytes of `kernel` from a committed ncu summary, if any:
+    a line 'traffic_bytes_per_launch <kernel> <bytes>' in profiles/*.md."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for fn in sorted(os.listdir(pdir)):
+        if not fn.endswith((".md", ".txt")):
+            continue
+        for line in open(os.path.join(pdir, fn)):
+            parts = line.strip().strip("`").split()
+            if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == kernel:
+                return float(parts[2])
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, w, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from model_mosaic_b200.processing.tomo import TomoReal
+    from model_mosaic_b200.processing.propagation import Propagation
+    from model_mosaic_b200.phantom import ellipsoid_volume_torch
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    n, nz, T = w["n"], w["nz"], w["ntheta"]
+    theta = np.linspace(0, w["theta_max"], T, endpoint=False).astype(np.float32)
+    wavelength = 1.24e-9 / w["energy_kev"]
+    inv_norm = float(np.float32(1.0 / np.sqrt(n / T)))       # step3_propagation.py:82,182
+    inv_beta = float(np.float32(1.0 / BETA_RATIO))
+
+    tomo = TomoReal(n, nz, theta)
+    prop = Propagation(n, nz, T, 1, wavelength, w["voxelsize"], [w["distance"]])
+    obj = ellipsoid_volume_torch(n, nz, seed=rank, device=dev)        # each rank: its own slab
+    sino = torch.empty((T, nz, n), dtype=torch.float32, device=dev)
+    inten = torch.empty((T, nz, n), dtype=torch.float32, device=dev)
+    rec = torch.empty((nz, n, n), dtype=torch.float32, device=dev)
+    if not args.no_rt:
+        tomo.prepare_rt()
+
+    def step():
+        tomo.R_into(obj, sino)
+        prop.intensity_into(sino, inten, inv_norm, inv_beta)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    # -- timed region: K steps, stage timers on the launching stream ----------
+    tomo.set_timing(True)
+    prop.set_timing(True)
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with Clocks(local_rank) as clk:
+        torch.cuda.nvtx.range_push("timed_step")
+        e0.record(st)
+        for _ in range(args.steps):
+            step()
+        e1.record(st)
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+    barrier()
+    ms_step = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    tstages, tk = tomo.timing()
+    pstages, pk = prop.timing()
+    tomo.set_timing(False)
+    prop.set_timing(False)
+
+    # -- adjoint RT on the same data (reported beside the step) --------------
+    ms_rt, rtstages = None, {}
+    if not args.no_rt:
+        for _ in range(max(1, args.warmup // 2)):
+            tomo.RT_into(sino, rec)
+        tomo.set_timing(True)
+        barrier()
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("timed_rt")
+        e0.record(st)
+        for _ in range(args.steps):
+            tomo.RT_into(sino, rec)
+        e1.record(st)
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+        ms_rt = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        rtstages, _ = tomo.timing()
+        tomo.set_timing(False)
+
+    # -- end to end through the public API: pinned host in, host out ---------
+    obj_h = obj.cpu().pin_memory()
+    out_h = torch.empty((T, nz, n), dtype=torch.float32).pin_memory()
+    obj_d = torch.empty_like(obj)
+
+    def e2e_step():
+        obj_d.copy_(obj_h, non_blocking=True)
+        tomo.R_into(obj_d, sino)
+        prop.intensity_into(sino, inten, inv_norm, inv_beta)
+        out_h.copy_(inten, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.nvtx.range_push("timed_e2e")
+    e0.record(st)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(st)
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+
+    V = nz * n * n
+    units = world * V * T
+    value = units / (ms_step * 1e-3) / 1e9
+    K = args.steps
+    r_ms = sum(v[0] for k, v in tstages.items() if v[1]) / K
+    d_ms = sum(v[0] for v in pstages.values()) / K
+
+    # roofline of the dominant own kernel in the step
+    P = T * nz * n
+    H = 2 * n * (n + 1) * nz
+    Kh = n // 2 + 1
+    alg = {  # algorithmic bytes per launch
+        "gather": 8 * H + 8 * Kh * T * nz,
+        "pad_phi": 4 * V + 8 * V,
+        "transpose_in": 2 * 8 * nz * n * (n + 1),
+        "y_pass": 4 * P + 8 * P,
+        "x_pass": 8 * P + 4 * P,
+    }
+    own = {"gather": tstages["gather"], "pad_phi": tstages["pad_phi"],
+           "transpose_in": tstages["transpose_in"], "y_pass": pstages["y_pass"], "x_pass": pstages["x_pass"]}
+    top = max(own, key=lambda k: own[k][0])
+    t_launch = own[top][0] / max(1, own[top][1])
+    peak, peak_kind = peaks()
+    achieved = alg[top] / (t_launch * 1e-3) / 1e9
+    kname = {"gather": "k_gather", "pad_phi": "k_pad_phi", "transpose_in": "k_transpose_in",
+             "y_pass": "k_ypass", "x_pass": "k_xpass"}[top]
+    traffic = profile_traffic(kname)
+    step_bytes = sum(alg.values()) - alg["pad_phi"] - alg["transpose_in"]    # B_R-like + B_D
+    roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak,
+            "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": traffic, "alg_bytes_per_launch": alg[top], "ms_per_launch": round(t_launch, 4)}
+
+    line = {
+        "metric": "R/RT Gvox·angle/s", "value": round(value, 3), "unit": "Gvox·angle/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: 10 seeded random ellipsoids per slab (values in [1e-7, 1e-6], beta = delta/100)",
+        "config": {"workload": workload_desc(w, args.workload), "n": n, "nz_per_rank": nz, "ntheta": T,
+                   "l2": "inputs larger than L2 (volume %.2f GB, sinogram %.2f GB per rank); no flush"
+                         % (4 * V / 1e9, 4 * P / 1e9),
+                   "parallelism": f"{world} ranks x independent slabs"},
+        "roofline": roof,
+        "gpu_launches": int(tk + pk),
+        "ops": {"R_ms": round(r_ms, 4), "D_ms": round(d_ms, 4), "RT_ms": round(ms_rt, 4) if ms_rt else None,
+                "R_gvox_angle_s": round(V * T / (r_ms * 1e-3) / 1e9, 3) if r_ms else None,
+                "RT_gvox_angle_s": round(world * V * T / (ms_rt * 1e-3) / 1e9, 3) if ms_rt else None,
+                "D_gpix_s": round(P / (d_ms * 1e-3) / 1e9, 3) if d_ms else None,
+                "step_frac_of_hbm": round(step_bytes / (ms_step * 1e-3) / 1e9 / peak, 4),
+                "stages_ms": {k: round(v[0] / K, 4) for k, v in {**tstages, **pstages}.items() if v[1]},
+                "rt_stages_ms": {k: round(v[0] / K, 4) for k, v in rtstages.items() if v[1] and k != "table_build"}},
+        "e2e": {"value": round(units / (ms_e2e * 1e-3) / 1e9, 3), "unit": "Gvox·angle/s",
+                "ms_per_step": round(ms_e2e, 4), "h2d_bytes_per_step": int(4 * V),
+                "d2h_bytes_per_step": int(4 * P)},
+        "clocks": clk.summary(),
+    }
+    return line
+
+
+# ---------------------------------------------------------------- CPU (reference kernels on the host)
+def cpu_sample(w, slices=1, frames=32, cores=None):
+    """Time the reference's kernels + restated glue on a bounded sample and
+    scale to one full step.  Returns (seconds per full step, description)."""
+    from oracle.refkernels import RefTomoReal, RefPropagation, available
+    from model_mosaic_b200.phantom import ellipsoid_volume
+    cores = cores or os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    n, nz, T = w["n"], w["nz"], w["ntheta"]
+    theta = np.linspace(0, w["theta_max"], T, endpoint=False).astype(np.float32)
+    x = ellipsoid_volume(n, nz, seed=0, z0=nz // 2, z1=nz // 2 + slices)
+    tomo = RefTomoReal(n, slices, theta, workers=cores)
+    wavelength = 1.24e-9 / w["energy_kev"]
+    prop = RefPropagation(n, nz, frames, 1, wavelength, w["voxelsize"], [w["distance"]], workers=cores)
+    frame = np.ascontiguousarray(
+        np.broadcast_to(ellipsoid_volume(n, 1, seed=1)[0][:nz][None], (frames, nz, n)).astype(np.float32))
+    t0 = time.perf_counter()
+    tomo.R(x)
+    t1 = time.perf_counter()
+    inv_norm = np.float32(1.0 / np.sqrt(n / T))
+    phase = frame * inv_norm
+    psi = (np.exp(-phase / BETA_RATIO) * (np.cos(phase) + 1j * np.sin(phase))).astype(np.complex64)
+    u = prop.D(psi, 0)
+    _ = (u.real * u.real + u.imag * u.imag)
+    t2 = time.perf_counter()
+    t_step = (t1 - t0) * (nz / slices) + (t2 - t1) * (T / frames)
+    kind = "reference" if available() else "port"
+    desc = (f"R of {slices} of {nz} slices and psi/D/|.|^2 of {frames} of {T} frames, scaled linearly "
+            f"to the full step; reference kernels (processing/kernels.py) built for the host with "
+            f"OpenMP, SciPy FFT workers={cores}")
+    return t_step, desc, kind, cores
+
+
+def run_reference(args, w):
+    n, nz, T = w["n"], w["nz"], w["ntheta"]
+    V = nz * n * n
+    for _ in range(args.warmup):
+        cpu_sample(w)
+    ts = []
+    desc = kind = cores = None
+    for _ in range(args.steps):
+        t, desc, kind, cores = cpu_sample(w)
+        ts.append(t)
+    t = statistics.median(ts)
+    value = V * T / t / 1e9
+    return {"metric": "R/RT Gvox·angle/s", "value": round(value, 5), "unit": "Gvox·angle/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: 10 seeded random ellipsoids (values in [1e-7, 1e-6], beta = delta/100)",
+            "config": {"workload": workload_desc(w, args.workload), "n": n, "nz_per_rank": nz, "ntheta": T},
+            "cpu_baseline": {"value": round(value, 5), "unit": "Gvox·angle/s", "cores": cores, "kind": kind,
+                             "sample": desc},
+            "e2e": {"value": round(value, 5), "unit": "Gvox·angle/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="production")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-rt", action="store_true", help="skip the adjoint (no scatter table)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    w = WORKLOADS[args.workload]
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, w)), flush=True)
+        return
+
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        line = run_ours(args, w, rank, world, local_rank)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            t, desc, kind, cores = cpu_sample(w)
+            V = w["nz"] * w["n"] ** 2
+            line["cpu_baseline"] = {"value": round(V * w["ntheta"] / t / 1e9, 5), "unit": "Gvox·angle/s",
+                                    "cores": cores, "kind": kind, "sample": desc}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

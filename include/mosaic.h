@@ -76,6 +76,18 @@ int mm_tomo_prepare_rt(mm_tomo* h, void* stream);
 /* Bytes of device workspace the handle holds now. */
 size_t mm_tomo_workspace_bytes(const mm_tomo* h);
 
+/* Per-stage CUDA-event timing (tracing; no reference counterpart -- the
+ * reference times whole stages with perf_counter, step2_radon.py:186-197).
+ * set_timing(1) resets and starts recording events around every stage on the
+ * call's stream; get_timing waits for them and returns, for up to nstages
+ * stages, the summed milliseconds and call counts, and the number of this
+ * library's own kernel launches since timing was switched on.
+ * Tomo stages: 0 pad+phi, 1 x-R2C, 2 transpose in, 3 y-FFT, 4 gather,
+ *   5 r-C2R (+ slice crop), 6 r-R2C (RT), 7 scatter, 8 y-IFFT, 9 transpose out,
+ *   10 x-C2R, 11 crop*phi, 12 scatter-table build, 13 complex-RT prologue. */
+int mm_tomo_set_timing(mm_tomo* h, int on);
+int mm_tomo_get_timing(mm_tomo* h, double* ms, long long* calls, int nstages, long long* kernels);
+
 /* ---- Fresnel propagator -------------------------------------------------
  * mm_prop_create replaces Propagation.__init__(n, nz, ntheta, ndist,
  *   wavelength, voxelsize, distance) (processing/propagation.py:18-35) and
@@ -101,6 +113,10 @@ int mm_prop_DT(mm_prop* h, const void* g, void* out, int ntheta, int j, void* st
  *   (_abs2_c64_to_f32, :105-110) -> intensity (ntheta, nz, n) f32. */
 int mm_prop_intensity(mm_prop* h, const float* proj, float inv_norm, float inv_beta_ratio,
                       float* intensity, int ntheta, int j, void* stream);
+
+/* Stage timing as for mm_tomo_*_timing.  Stages: 0 y-pass (columns), 1 x-pass (rows). */
+int mm_prop_set_timing(mm_prop* h, int on);
+int mm_prop_get_timing(mm_prop* h, double* ms, long long* calls, int nstages, long long* kernels);
 
 #ifdef __cplusplus
 }

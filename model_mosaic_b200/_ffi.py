@@ -49,7 +49,13 @@ def _declare(L):
     L.mm_prop_D.argtypes = [p, p, p, i, i, p]
     L.mm_prop_DT.argtypes = [p, p, p, i, i, p]
     L.mm_prop_intensity.argtypes = [p, p, f, f, p, i, i, p]
-    for name in ("mm_tomo_create", "mm_tomo_destroy", "mm_tomo_R", "mm_tomo_RT", "mm_tomo_prepare_rt",
+    dp, llp = C.POINTER(C.c_double), C.POINTER(C.c_longlong)
+    L.mm_tomo_set_timing.argtypes = [p, i]
+    L.mm_tomo_get_timing.argtypes = [p, dp, llp, i, llp]
+    L.mm_prop_set_timing.argtypes = [p, i]
+    L.mm_prop_get_timing.argtypes = [p, dp, llp, i, llp]
+    for name in ("mm_tomo_set_timing", "mm_tomo_get_timing", "mm_prop_set_timing", "mm_prop_get_timing",
+                 "mm_tomo_create", "mm_tomo_destroy", "mm_tomo_R", "mm_tomo_RT", "mm_tomo_prepare_rt",
                  "mm_prop_create", "mm_prop_destroy", "mm_prop_D", "mm_prop_DT", "mm_prop_intensity"):
         getattr(L, name).restype = i
     return L
@@ -87,3 +93,18 @@ def check(status: int, what: str = "") -> None:
     if status == MM_ETIMEOUT:
         raise MosaicTimeout(status, msg)
     raise MosaicError(status, msg)
+
+
+TOMO_STAGES = ("pad_phi", "x_r2c", "transpose_in", "y_fft", "gather", "r_c2r", "r_r2c", "scatter",
+               "y_ifft", "transpose_out", "x_c2r", "crop_phi", "table_build", "complex_prologue")
+PROP_STAGES = ("y_pass", "x_pass")
+
+
+def read_timing(get, handle, names):
+    """{stage: (ms, calls)} and own-kernel launch count from mm_*_get_timing."""
+    k = len(names)
+    ms = (C.c_double * k)()
+    calls = (C.c_longlong * k)()
+    kern = C.c_longlong()
+    check(get(handle, ms, calls, k, C.byref(kern)))
+    return {names[i]: (ms[i], calls[i]) for i in range(k)}, kern.value

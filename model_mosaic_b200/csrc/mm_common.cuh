@@ -10,7 +10,69 @@
 
 #include "../../include/mosaic.h"
 
+#include <vector>
+
 namespace mm {
+
+// Optional per-stage CUDA-event timing of a handle's launches (off by
+// default).  begin()/end() bracket one stage on the caller's stream; read()
+// waits for the recorded events and adds their elapsed times per stage.
+struct StageTimer {
+    static constexpr int kMax = 16;
+    bool on = false;
+    double ms[kMax] = {0};
+    long long calls[kMax] = {0};
+    long long kernels = 0;  // launches of this library's own kernels while on
+    struct Rec { int stage; cudaEvent_t a, b; };
+    std::vector<Rec> pending;
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t cur_a = nullptr;
+    int cur_stage = -1;
+
+    cudaEvent_t take() {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void begin(int stage, cudaStream_t st) {
+        if (!on) return;
+        cur_stage = stage;
+        cur_a = take();
+        cudaEventRecord(cur_a, st);
+    }
+    void end(cudaStream_t st, int own_kernels) {
+        if (!on || cur_stage < 0) return;
+        cudaEvent_t b = take();
+        cudaEventRecord(b, st);
+        pending.push_back({cur_stage, cur_a, b});
+        kernels += own_kernels;
+        cur_stage = -1;
+        if (pending.size() > 4096) read();  // bound the event backlog
+    }
+    void read() {
+        for (auto& r : pending) {
+            float t = 0.f;
+            cudaEventSynchronize(r.b);
+            cudaEventElapsedTime(&t, r.a, r.b);
+            ms[r.stage] += t;
+            calls[r.stage] += 1;
+            pool.push_back(r.a);
+            pool.push_back(r.b);
+        }
+        pending.clear();
+    }
+    void reset() {
+        read();
+        for (int i = 0; i < kMax; ++i) { ms[i] = 0; calls[i] = 0; }
+        kernels = 0;
+    }
+    void release() {
+        read();
+        for (cudaEvent_t e : pool) cudaEventDestroy(e);
+        pool.clear();
+    }
+};
 
 void set_error(const char* fmt, ...);
 const char* cufft_name(cufftResult r);

@@ -31,10 +31,13 @@ struct mm_prop {
     int n = 0, nz = 0, ntheta = 0, ndist = 0;
     float2* Kx = nullptr;   // (ndist, 2n)
     float2* Ky = nullptr;   // (ndist, 2nz)
-    float2* twx = nullptr;  // (2n)  exp(-2 pi i k / 2n)
-    float2* twy = nullptr;  // (2nz)
+    // inter-step twiddles W_L^(k1*n2) of L = R1*R2 as two tables laid out so
+    // that the lanes of a warp read consecutive entries: A[k1][n2], B[n2][k1]
+    float2* twx = nullptr;  // (2 * 2n)  x: A then B
+    float2* twy = nullptr;  // (2 * 2nz) y: A then B
     float2* mid = nullptr;  // (ntheta, nz, n)
     size_t ws_bytes = 0;
+    mm::StageTimer tm;
 };
 
 namespace {
@@ -64,6 +67,27 @@ __global__ void __launch_bounds__(CW * Split<L>::R2) k_ypass(const void* __restr
     const int x = blockIdx.x * CW + c;
     const bool live = x < n;
     const long plane = (long)blockIdx.y * nz * n;
+    const float2* twA = tw;          // [R1][R2]
+    const float2* twB = tw + L;      // [R2][R1]
+    // stage the nz source rows of this column block once (psi built here);
+    // the mirror padding then reads each of them twice from shared memory
+    for (int r = g; r < nz; r += R2) {
+        float2 a = make_float2(0.f, 0.f);
+        if (live) {
+            const long off = plane + (long)r * n + x;
+            if (IN == 0) {
+                a = __ldg(static_cast<const float2*>(src) + off);
+            } else {
+                const float ph = __ldg(static_cast<const float*>(src) + off) * s;
+                const float at = expf(-ph * ib);
+                float sn, cs;
+                sincosf(ph, &sn, &cs);
+                a = make_float2(at * cs, at * sn);
+            }
+        }
+        sm[r * CW + c] = a;
+    }
+    __syncthreads();
     float2 v[R1];
 #pragma unroll
     for (int n1 = 0; n1 < R1; ++n1) {
@@ -76,25 +100,13 @@ __global__ void __launch_bounds__(CW * Split<L>::R2) k_ypass(const void* __restr
             r = idx - nz / 2;
             zero = r < 0 || r >= nz;
         }
-        float2 a = make_float2(0.f, 0.f);
-        if (live && !zero) {
-            const long off = plane + (long)r * n + x;
-            if (IN == 0) {
-                a = __ldg(static_cast<const float2*>(src) + off);
-            } else {
-                const float ph = __ldg(static_cast<const float*>(src) + off) * s;
-                const float at = expf(-ph * ib);
-                float sn, cs;
-                sincosf(ph, &sn, &cs);
-                a = make_float2(at * cs, at * sn);
-            }
-        }
-        v[n1] = a;
+        v[n1] = zero ? make_float2(0.f, 0.f) : sm[r * CW + c];
     }
+    __syncthreads();
     reg_fft<R1, false>(v);
 #pragma unroll
     for (int k1 = 1; k1 < R1; ++k1)
-        if (g) v[k1] = cmul(v[k1], __ldg(tw + g * k1));
+        if (g) v[k1] = cmul(v[k1], __ldg(twA + k1 * R2 + g));
 #pragma unroll
     for (int k1 = 0; k1 < R1; ++k1) sm[(k1 * R2 + g) * CW + c] = v[k1];
     __syncthreads();
@@ -113,7 +125,7 @@ __global__ void __launch_bounds__(CW * Split<L>::R2) k_ypass(const void* __restr
         reg_fft<R2, true>(u);
 #pragma unroll
         for (int m2 = 1; m2 < R2; ++m2)
-            if (k1) u[m2] = cmulc(u[m2], __ldg(tw + k1 * m2));
+            if (k1) u[m2] = cmulc(u[m2], __ldg(twB + m2 * R1 + k1));
 #pragma unroll
         for (int m2 = 0; m2 < R2; ++m2) sm[(k1 * R2 + m2) * CW + c] = u[m2];
     }
@@ -152,6 +164,8 @@ __global__ void __launch_bounds__(RPB * Split<L>::R2) k_xpass(const float2* __re
     const bool live = row < rows;
     float2* S = sm + rr * R1 * P;
     const float2* in = src + row * n;
+    const float2* twA = tw;          // [R1][R2]
+    const float2* twB = tw + L;      // [R2][R1]
     float2 v[R1];
 #pragma unroll
     for (int n1 = 0; n1 < R1; ++n1) {
@@ -169,7 +183,7 @@ __global__ void __launch_bounds__(RPB * Split<L>::R2) k_xpass(const float2* __re
     reg_fft<R1, false>(v);
 #pragma unroll
     for (int k1 = 1; k1 < R1; ++k1)
-        if (g) v[k1] = cmul(v[k1], __ldg(tw + g * k1));
+        if (g) v[k1] = cmul(v[k1], __ldg(twA + k1 * R2 + g));
 #pragma unroll
     for (int k1 = 0; k1 < R1; ++k1) S[k1 * P + g] = v[k1];
     __syncthreads();
@@ -188,7 +202,7 @@ __global__ void __launch_bounds__(RPB * Split<L>::R2) k_xpass(const float2* __re
         reg_fft<R2, true>(u);
 #pragma unroll
         for (int m2 = 1; m2 < R2; ++m2)
-            if (k1) u[m2] = cmulc(u[m2], __ldg(tw + k1 * m2));
+            if (k1) u[m2] = cmulc(u[m2], __ldg(twB + m2 * R1 + k1));
 #pragma unroll
         for (int m2 = 0; m2 < R2; ++m2) S[k1 * P + m2] = u[m2];
     }
@@ -221,7 +235,7 @@ __global__ void __launch_bounds__(RPB * Split<L>::R2) k_xpass(const float2* __re
 
 // ---------------------------------------------------------------- launch
 template <int L, int IN, bool ADJ>
-int launch_y(const mm_prop* h, const void* src, int ntheta, int j, float s, float ib, cudaStream_t st) {
+int launch_y(mm_prop* h, const void* src, int ntheta, int j, float s, float ib, cudaStream_t st) {
     constexpr int R2 = Split<L>::R2;
     constexpr int CW0 = 256 / R2;
     constexpr int CW = CW0 < 4 ? 4 : (CW0 > 32 ? 32 : CW0);
@@ -229,13 +243,15 @@ int launch_y(const mm_prop* h, const void* src, int ntheta, int j, float s, floa
     auto kern = k_ypass<L, CW, IN, ADJ>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 block(CW, R2), grid((h->n + CW - 1) / CW, ntheta);
+    h->tm.begin(0, st);
     kern<<<grid, block, smem, st>>>(src, h->mid, h->Ky + (size_t)j * 2 * h->nz, h->twy, h->n, h->nz, s, ib);
     MM_LAUNCHED();
+    h->tm.end(st, 1);
     return MM_OK;
 }
 
 template <int L, int OUT, bool ADJ>
-int launch_x(const mm_prop* h, void* dst, int ntheta, int j, cudaStream_t st) {
+int launch_x(mm_prop* h, void* dst, int ntheta, int j, cudaStream_t st) {
     constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2;
     constexpr int RPB = R2 >= 128 ? 1 : 128 / R2;
     const size_t smem = (size_t)RPB * R1 * (R2 + 1) * sizeof(float2);
@@ -243,13 +259,15 @@ int launch_x(const mm_prop* h, void* dst, int ntheta, int j, cudaStream_t st) {
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long rows = (long)ntheta * h->nz;
     dim3 block(R2, RPB), grid((unsigned)((rows + RPB - 1) / RPB));
+    h->tm.begin(1, st);
     kern<<<grid, block, smem, st>>>(h->mid, dst, h->Kx + (size_t)j * 2 * h->n, h->twx, h->n, rows);
     MM_LAUNCHED();
+    h->tm.end(st, 1);
     return MM_OK;
 }
 
 template <int IN, bool ADJ>
-int dispatch_y(const mm_prop* h, const void* src, int ntheta, int j, float s, float ib, cudaStream_t st) {
+int dispatch_y(mm_prop* h, const void* src, int ntheta, int j, float s, float ib, cudaStream_t st) {
     switch (2 * h->nz) {
         case 4: return launch_y<4, IN, ADJ>(h, src, ntheta, j, s, ib, st);
         case 8: return launch_y<8, IN, ADJ>(h, src, ntheta, j, s, ib, st);
@@ -267,7 +285,7 @@ int dispatch_y(const mm_prop* h, const void* src, int ntheta, int j, float s, fl
 }
 
 template <int OUT, bool ADJ>
-int dispatch_x(const mm_prop* h, void* dst, int ntheta, int j, cudaStream_t st) {
+int dispatch_x(mm_prop* h, void* dst, int ntheta, int j, cudaStream_t st) {
     switch (2 * h->n) {
         case 4: return launch_x<4, OUT, ADJ>(h, dst, ntheta, j, st);
         case 8: return launch_x<8, OUT, ADJ>(h, dst, ntheta, j, st);
@@ -293,6 +311,7 @@ int check_call(const mm_prop* h, const void* a, const void* b, int ntheta, int j
 }
 
 void destroy(mm_prop* h) {
+    h->tm.release();
     void* bufs[] = {h->Kx, h->Ky, h->twx, h->twy, h->mid};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -311,11 +330,21 @@ void chirp(std::vector<float2>& out, int len, double voxelsize, double wavelengt
     }
 }
 
+// Two layouts of W_len^(i*j), i < R1, j < R2 (R1 >= R2 as in mmfft::Split):
+// out[i*R2 + j] and out[len + j*R1 + i].
 void twiddles(std::vector<float2>& out, int len) {
-    for (int k = 0; k < len; ++k) {
-        const double a = -2.0 * M_PI * k / len;
-        out[k] = make_float2((float)cos(a), (float)sin(a));
-    }
+    int r2 = 1;
+    while (r2 * r2 < len) r2 <<= 1;
+    if (r2 * r2 > len) r2 >>= 1;
+    const int r1 = len / r2;
+    out.assign(2 * (size_t)len, make_float2(0.f, 0.f));
+    for (int i = 0; i < r1; ++i)
+        for (int j = 0; j < r2; ++j) {
+            const double a = -2.0 * M_PI * (double)((long)i * j % len) / len;
+            const float2 w = make_float2((float)cos(a), (float)sin(a));
+            out[(size_t)i * r2 + j] = w;
+            out[len + (size_t)j * r1 + i] = w;
+        }
 }
 
 }  // namespace
@@ -336,7 +365,7 @@ extern "C" int mm_prop_create(int n, int nz, int ntheta, int ndist, double wavel
     h->nz = nz;
     h->ntheta = ntheta;
     h->ndist = ndist;
-    std::vector<float2> kx((size_t)ndist * 2 * n), ky((size_t)ndist * 2 * nz), tx(2 * n), ty(2 * nz), tmp;
+    std::vector<float2> kx((size_t)ndist * 2 * n), ky((size_t)ndist * 2 * nz), tx, ty, tmp;
     for (int j = 0; j < ndist; ++j) {
         tmp.assign(2 * n, make_float2(0, 0));
         chirp(tmp, 2 * n, voxelsize, wavelength, distance_host[j]);
@@ -400,4 +429,22 @@ extern "C" int mm_prop_intensity(mm_prop* h, const float* proj, float inv_norm, 
     cudaStream_t st = (cudaStream_t)stream;
     MM_TRY((dispatch_y<1, false>(h, proj, ntheta, j, inv_norm, inv_beta_ratio, st)));
     return dispatch_x<1, false>(h, intensity, ntheta, j, st);
+}
+
+extern "C" int mm_prop_set_timing(mm_prop* h, int on) {
+    MM_REQUIRE(h != nullptr, "mm_prop_set_timing: NULL handle");
+    h->tm.reset();
+    h->tm.on = on != 0;
+    return MM_OK;
+}
+
+extern "C" int mm_prop_get_timing(mm_prop* h, double* ms, long long* calls, int nstages, long long* kernels) {
+    MM_REQUIRE(h != nullptr, "mm_prop_get_timing: NULL handle");
+    h->tm.read();
+    for (int i = 0; i < nstages && i < mm::StageTimer::kMax; ++i) {
+        if (ms) ms[i] = h->tm.ms[i];
+        if (calls) calls[i] = h->tm.calls[i];
+    }
+    if (kernels) *kernels = h->tm.kernels;
+    return MM_OK;
 }

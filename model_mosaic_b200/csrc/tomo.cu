@@ -56,6 +56,7 @@ struct mm_tomo {
     float* ypad = nullptr;       // (T, zs, n) real sino padded in z (nz < zs)
     float2* yc = nullptr;        // (T, zs, n) complex sino spectrum (complex RT)
     size_t ws_bytes = 0;
+    mm::StageTimer tm;
 };
 
 namespace {
@@ -569,6 +570,7 @@ int launch_scatter(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) {
 
 int build_csr(mm_tomo* h, cudaStream_t st) {
     if (h->csr_ready) return MM_OK;
+    h->tm.begin(12, st);
     const int n = h->n, T = h->ntheta, M = h->m, L = 2 * M + 1;
     const long nent = (long)T * h->K * L * L;
     const long ncells = 2L * n * (n + 1);
@@ -624,6 +626,7 @@ int build_csr(mm_tomo* h, cudaStream_t st) {
     }
     h->nnz = nent;
     h->csr_ready = true;
+    h->tm.end(st, 3);
     return MM_OK;
 }
 
@@ -640,6 +643,7 @@ int ensure_rt(mm_tomo* h, cudaStream_t st) {
 }
 
 void destroy(mm_tomo* h) {
+    h->tm.release();
     cufftHandle all[6] = {h->plan_xr2c, h->plan_xc2r, h->plan_y, h->plan_rc2r, h->plan_rr2c, h->plan_rc2c};
     for (cufftHandle p : all)
         if (p) cufftDestroy(p);
@@ -747,6 +751,7 @@ extern "C" int mm_tomo_R(mm_tomo* h, const float* obj, float* sino, int nz, void
     MM_REQUIRE(((uintptr_t)obj % 4) == 0 && ((uintptr_t)sino % 4) == 0, "mm_tomo_R: misaligned array");
     cudaStream_t st = (cudaStream_t)stream;
     const int n = h->n, zs = h->zs, T = h->ntheta;
+    h->tm.begin(0, st);
     if (h->y_dirty) {  // rows [0, n/2) and [3n/2, 2n) of Y are the y zero padding
         const size_t half = (size_t)(n / 2) * (n + 1) * zs * sizeof(float2);
         MM_CUDA(cudaMemsetAsync(h->Y, 0, half, st));
@@ -755,14 +760,24 @@ extern "C" int mm_tomo_R(mm_tomo* h, const float* obj, float* sino, int nz, void
     }
     k_pad_phi<<<(unsigned)((long)zs * n), kThreads, 0, st>>>(obj, h->P, h->d_phi1, h->phi_scale, n, nz);
     MM_LAUNCHED();
+    h->tm.end(st, 1);
+    h->tm.begin(1, st);
     MM_CUFFT(cufftSetStream(h->plan_xr2c, st));
     MM_CUFFT(cufftExecR2C(h->plan_xr2c, h->P, (cufftComplex*)h->X));
+    h->tm.end(st, 0);
+    h->tm.begin(2, st);
     dim3 tb(32, 8), tg((n + 1 + 31) / 32, (zs + 31) / 32, n);
     k_transpose_in<<<tg, tb, 0, st>>>(h->X, h->Y, n, zs);
     MM_LAUNCHED();
+    h->tm.end(st, 1);
+    h->tm.begin(3, st);
     MM_CUFFT(cufftSetStream(h->plan_y, st));
     MM_CUFFT(cufftExecC2C(h->plan_y, (cufftComplex*)h->Y, (cufftComplex*)h->F, CUFFT_FORWARD));
+    h->tm.end(st, 0);
+    h->tm.begin(4, st);
     MM_TRY(launch_gather(h, st));
+    h->tm.end(st, 1);
+    h->tm.begin(5, st);
     float* dst = sino;
     if (nz < zs) {
         if (!h->sino_tmp) MM_TRY(alloc(h, &h->sino_tmp, (size_t)T * zs * n, "padded sinogram"));
@@ -774,6 +789,7 @@ extern "C" int mm_tomo_R(mm_tomo* h, const float* obj, float* sino, int nz, void
         k_copy_z<<<(unsigned)((long)T * nz), kThreads, 0, st>>>(h->sino_tmp, sino, n, zs, nz, nz);
         MM_LAUNCHED();
     }
+    h->tm.end(st, nz < zs ? 1 : 0);
     return MM_OK;
 }
 
@@ -785,17 +801,25 @@ extern "C" int mm_tomo_prepare_rt(mm_tomo* h, void* stream) {
 namespace {
 // scatter + IFFT along v + transposed C2R along x + crop*phi for one real
 // run whose line spectra are in Q = h->Hh.  OUT selects the output part.
-int rt_tail(mm_tomo* h, void* obj, int out, cudaStream_t st) {
+int rt_tail(mm_tomo* h, cudaStream_t st) {
     const int n = h->n, zs = h->zs;
+    h->tm.begin(7, st);
     MM_TRY(launch_scatter(h, h->Hh, h->F, st));
+    h->tm.end(st, 1);
+    h->tm.begin(8, st);
     MM_CUFFT(cufftSetStream(h->plan_y, st));
     MM_CUFFT(cufftExecC2C(h->plan_y, (cufftComplex*)h->F, (cufftComplex*)h->Y, CUFFT_INVERSE));
     h->y_dirty = true;
+    h->tm.end(st, 0);
+    h->tm.begin(9, st);
     dim3 tb(32, 8), tg((n + 1 + 31) / 32, (zs + 31) / 32, n);
     k_transpose_out<<<tg, tb, 0, st>>>(h->Y, h->X, n, zs);
     MM_LAUNCHED();
+    h->tm.end(st, 1);
+    h->tm.begin(10, st);
     MM_CUFFT(cufftSetStream(h->plan_xc2r, st));
     MM_CUFFT(cufftExecC2R(h->plan_xc2r, (cufftComplex*)h->X, h->P));
+    h->tm.end(st, 0);
     return MM_OK;
 }
 }  // namespace
@@ -812,6 +836,7 @@ extern "C" int mm_tomo_RT(mm_tomo* h, const void* sino, int dtype, void* obj, in
     const int n = h->n, zs = h->zs, T = h->ntheta;
     const unsigned rows = (unsigned)((long)nz * n);
     if (dtype == MM_F32) {
+        h->tm.begin(6, st);
         const float* y = static_cast<const float*>(sino);
         if (nz < zs) {
             if (!h->ypad) MM_TRY(alloc(h, &h->ypad, (size_t)T * zs * n, "padded sinogram"));
@@ -821,9 +846,12 @@ extern "C" int mm_tomo_RT(mm_tomo* h, const void* sino, int dtype, void* obj, in
         }
         MM_CUFFT(cufftSetStream(h->plan_rr2c, st));
         MM_CUFFT(cufftExecR2C(h->plan_rr2c, (cufftReal*)y, (cufftComplex*)h->Hh));
-        MM_TRY(rt_tail(h, obj, 0, st));
+        h->tm.end(st, nz < zs ? 1 : 0);
+        MM_TRY(rt_tail(h, st));
+        h->tm.begin(11, st);
         k_crop_phi<0><<<rows, kThreads, 0, st>>>(h->P, obj, h->d_phi1, h->phi_scale, n);
         MM_LAUNCHED();
+        h->tm.end(st, 1);
         return MM_OK;
     }
     // complex64 sinogram: real and imaginary output parts are two real runs
@@ -834,6 +862,7 @@ extern "C" int mm_tomo_RT(mm_tomo* h, const void* sino, int dtype, void* obj, in
         MM_TRY(ensure_work(h, ws));
     }
     if (!h->yc) MM_TRY(alloc(h, &h->yc, (size_t)T * zs * n, "complex line spectra"));
+    h->tm.begin(13, st);
     const float2* y = static_cast<const float2*>(sino);
     if (nz < zs) {
         k_copy_z_c<<<(unsigned)((long)T * zs), kThreads, 0, st>>>(y, h->yc, n, nz, zs, nz);
@@ -842,18 +871,41 @@ extern "C" int mm_tomo_RT(mm_tomo* h, const void* sino, int dtype, void* obj, in
     }
     MM_CUFFT(cufftSetStream(h->plan_rc2c, st));
     MM_CUFFT(cufftExecC2C(h->plan_rc2c, (cufftComplex*)y, (cufftComplex*)h->yc, CUFFT_FORWARD));
+    h->tm.end(st, nz < zs ? 1 : 0);
     for (int part = 0; part < 2; ++part) {
+        h->tm.begin(6, st);
         if (part == 0)
             k_combine<0><<<(unsigned)((long)T * zs), kThreads, 0, st>>>(h->yc, h->Hh, n, T, zs);
         else
             k_combine<1><<<(unsigned)((long)T * zs), kThreads, 0, st>>>(h->yc, h->Hh, n, T, zs);
         MM_LAUNCHED();
-        MM_TRY(rt_tail(h, obj, part + 1, st));
+        h->tm.end(st, 1);
+        MM_TRY(rt_tail(h, st));
+        h->tm.begin(11, st);
         if (part == 0)
             k_crop_phi<1><<<rows, kThreads, 0, st>>>(h->P, obj, h->d_phi1, h->phi_scale, n);
         else
             k_crop_phi<2><<<rows, kThreads, 0, st>>>(h->P, obj, h->d_phi1, h->phi_scale, n);
         MM_LAUNCHED();
+        h->tm.end(st, 1);
     }
+    return MM_OK;
+}
+
+extern "C" int mm_tomo_set_timing(mm_tomo* h, int on) {
+    MM_REQUIRE(h != nullptr, "mm_tomo_set_timing: NULL handle");
+    h->tm.reset();
+    h->tm.on = on != 0;
+    return MM_OK;
+}
+
+extern "C" int mm_tomo_get_timing(mm_tomo* h, double* ms, long long* calls, int nstages, long long* kernels) {
+    MM_REQUIRE(h != nullptr, "mm_tomo_get_timing: NULL handle");
+    h->tm.read();
+    for (int i = 0; i < nstages && i < mm::StageTimer::kMax; ++i) {
+        if (ms) ms[i] = h->tm.ms[i];
+        if (calls) calls[i] = h->tm.calls[i];
+    }
+    if (kernels) *kernels = h->tm.kernels;
     return MM_OK;
 }

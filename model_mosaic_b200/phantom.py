@@ -50,3 +50,25 @@ def ellipsoid_volume(n, nz, seed=0, count=10, vmin=1e-7, vmax=1e-6, z0=0, z1=Non
             inside = (q[0] / axes[0]) ** 2 + (q[1] / axes[1]) ** 2 + (q[2] / axes[2]) ** 2 <= 1.0
             vol[iz - z0][inside] += np.float32(val)
     return vol
+
+
+def ellipsoid_volume_torch(n, nz, seed=0, count=10, vmin=1e-7, vmax=1e-6, device="cuda", zblock=16):
+    """Same seeded volume as ``ellipsoid_volume``, evaluated on the GPU
+    (float32 (nz, n, n) torch tensor); used for the large workloads."""
+    import torch
+    vol = torch.zeros((nz, n, n), dtype=torch.float32, device=device)
+    c = torch.arange(n, device=device, dtype=torch.float64) - n / 2 + 0.5
+    for (ctr, axes, rot, val) in ellipsoid_params(n, nz, seed, count, vmin, vmax):
+        inv = rot.T
+        for z0 in range(0, nz, zblock):
+            z1 = min(nz, z0 + zblock)
+            dz = (torch.arange(z0, z1, device=device, dtype=torch.float64) - nz / 2 + 0.5 - ctr[0])[:, None, None]
+            dy = (c - ctr[1])[None, :, None]
+            dx = (c - ctr[2])[None, None, :]
+            acc = None
+            for r in range(3):
+                q = inv[r, 0] * dz + inv[r, 1] * dy + inv[r, 2] * dx
+                t = (q / axes[r]) ** 2
+                acc = t if acc is None else acc + t
+            vol[z0:z1] += (acc <= 1.0).to(torch.float32) * float(np.float32(val))
+    return vol

@@ -90,6 +90,14 @@ class Propagation:
             out = out[0]
         return from_device(out, kind)
 
+    # -- per-stage CUDA-event timing ---------------------------------------------
+    def set_timing(self, on: bool = True):
+        _ffi.check(_ffi.lib().mm_prop_set_timing(self._handle(), int(bool(on))))
+
+    def timing(self):
+        """({stage: (ms, calls)}, own kernel launches) since set_timing(True)."""
+        return _ffi.read_timing(_ffi.lib().mm_prop_get_timing, self._handle(), _ffi.PROP_STAGES)
+
     # torch-native entry points (no copies, caller-provided outputs)
     def D_into(self, x: torch.Tensor, out: torch.Tensor, j=0):
         _ffi.check(_ffi.lib().mm_prop_D(self._handle(), C.c_void_p(x.data_ptr()), C.c_void_p(out.data_ptr()),

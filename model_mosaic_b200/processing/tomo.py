@@ -102,6 +102,14 @@ class TomoReal:
                                          C.c_void_p(stream_ptr(y.device))), "mm_tomo_RT")
         return from_device(out, kind)
 
+    # -- per-stage CUDA-event timing ---------------------------------------------
+    def set_timing(self, on: bool = True):
+        _ffi.check(_ffi.lib().mm_tomo_set_timing(self._handle(), int(bool(on))))
+
+    def timing(self):
+        """({stage: (ms, calls)}, own kernel launches) since set_timing(True)."""
+        return _ffi.read_timing(_ffi.lib().mm_tomo_get_timing, self._handle(), _ffi.TOMO_STAGES)
+
     # torch-native entry points used by the differentiable model (no copies)
     def R_into(self, x: torch.Tensor, out: torch.Tensor):
         _ffi.check(_ffi.lib().mm_tomo_R(self._handle(), C.c_void_p(x.data_ptr()), C.c_void_p(out.data_ptr()),

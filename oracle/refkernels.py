@@ -44,10 +44,26 @@ def _ptr(a):
     return a.ctypes.data_as(C.c_void_p)
 
 
+def _fft_backend(workers):
+    """numpy.fft (single thread) or scipy.fft with `workers` threads."""
+    if workers:
+        import functools
+        import scipy.fft as sf
+        class _F:
+            rfft2 = functools.partial(sf.rfft2, workers=workers)
+            ifft = functools.partial(sf.ifft, workers=workers)
+            fft = functools.partial(sf.fft, workers=workers)
+            ifft2 = functools.partial(sf.ifft2, workers=workers)
+            fft2 = functools.partial(sf.fft2, workers=workers)
+        return _F
+    return np.fft
+
+
 class RefTomoReal:
     """TomoReal (processing/tomo.py) with the reference gather kernels."""
 
-    def __init__(self, n, nz, theta):
+    def __init__(self, n, nz, theta, workers=0):
+        self.fft = _fft_backend(workers)
         self.n, self.nz = n, nz
         self.theta = np.ascontiguousarray(np.asarray(theta).astype(np.float32))
         self.ntheta = len(self.theta)
@@ -64,12 +80,12 @@ class RefTomoReal:
         nz = obj.shape[0]
         padded = np.zeros((nz, 2 * n, 2 * n), np.float32)
         padded[:, n // 2:3 * n // 2, n // 2:3 * n // 2] = obj.astype(np.float32) * self.phi
-        fde = np.ascontiguousarray(np.fft.rfft2(padded, axes=(-2, -1)).astype(np.complex64))
+        fde = np.ascontiguousarray(self.fft.rfft2(padded, axes=(-2, -1)).astype(np.complex64))
         sino = np.zeros((T, nz, n), np.complex64)
         lib().ref_launch_gather_rfft_full(n, T, nz, _ptr(sino), _ptr(fde), _ptr(self.theta),
                                           self.m, _ptr(self.mua), n, T, nz)
         sino *= self.c1d
-        sino = np.fft.ifft(sino, axis=-1).astype(np.complex64) * self.c1d
+        sino = self.fft.ifft(sino, axis=-1).astype(np.complex64) * self.c1d
         return np.ascontiguousarray(sino.real / 4).astype(np.float32)
 
     def RT(self, data):
@@ -127,7 +143,8 @@ class RefTomoLargeReal(RefTomoReal):
 class RefPropagation:
     """Propagation.D (processing/propagation.py:47-64) with pad_fwd."""
 
-    def __init__(self, n, nz, ntheta, ndist, wavelength, voxelsize, distance):
+    def __init__(self, n, nz, ntheta, ndist, wavelength, voxelsize, distance, workers=0):
+        self.fft = _fft_backend(workers)
         self.n, self.nz = n, nz
         self.fker = fresnel_kernel(n, nz, wavelength, voxelsize, list(distance)[:ndist], np.float32)
 
@@ -140,7 +157,7 @@ class RefPropagation:
         src = np.ascontiguousarray(psi.astype(np.complex64))
         pad = np.zeros((T, 2 * nz, 2 * n), np.complex64)
         lib().ref_launch_pad_fwd(2 * n, 2 * nz, T, _ptr(pad), _ptr(src), n, nz, T)
-        f = np.fft.fft2(pad, axes=(-2, -1)).astype(np.complex64) * self.fker[j]
-        f = np.fft.ifft2(f, axes=(-2, -1), norm="forward").astype(np.complex64)
+        f = self.fft.fft2(pad, axes=(-2, -1)).astype(np.complex64) * self.fker[j]
+        f = self.fft.ifft2(f, axes=(-2, -1), norm="forward").astype(np.complex64)
         res = np.ascontiguousarray(f[:, nz // 2:nz // 2 + nz, n // 2:n // 2 + n])
         return res[0] if added else res
