@@ -114,6 +114,19 @@ int mm_prop_DT(mm_prop* h, const void* g, void* out, int ntheta, int j, void* st
 int mm_prop_intensity(mm_prop* h, const float* proj, float inv_norm, float inv_beta_ratio,
                       float* intensity, int ntheta, int j, void* stream);
 
+/* Allocation-free Fresnel D for callers that cannot allocate device memory
+ *   while they run (their GPU memory is reserved up front by their own pool
+ *   allocator, so a cudaMalloc mid-run fails or stalls other work).  No
+ *   counterpart in the reference.  Same operator and layouts as mm_prop_D for
+ *   one distance, without a handle: the chirp/twiddle tables and the
+ *   intermediate live in one static 64 MiB device array per GPU, so
+ *   (ntheta*nz*n + 6*(n+nz)) * 8 bytes must fit in 64 MiB (MM_EINVAL
+ *   otherwise).  The first call on each device resolves that array's address;
+ *   make it before any stream capture.  Calls share the array: calls that
+ *   overlap on the GPU race and must be ordered by the caller. */
+int mm_prop_D_noalloc(int n, int nz, int ntheta, double wavelength, double voxelsize, double distance,
+                      const void* psi, void* out, void* stream);
+
 /* Stage timing as for mm_tomo_*_timing.  Stages: 0 y-pass (columns), 1 x-pass (rows). */
 int mm_prop_set_timing(mm_prop* h, int on);
 int mm_prop_get_timing(mm_prop* h, double* ms, long long* calls, int nstages, long long* kernels);

@@ -19,6 +19,7 @@
 
 #include <math.h>
 
+#include <mutex>
 #include <vector>
 
 using mm::dev_alloc;
@@ -447,4 +448,124 @@ extern "C" int mm_prop_get_timing(mm_prop* h, double* ms, long long* calls, int 
     }
     if (kernels) *kernels = h->tm.kernels;
     return MM_OK;
+}
+
+// ==========================================================================
+// Allocation-free Fresnel D.
+//
+// Some callers cannot allocate device memory at call time: a host program
+// whose GPU memory is entirely reserved up front by its own pool allocator
+// (an acquisition or streaming-reconstruction service, or a process where
+// another framework's caching allocator owns the device) sees cudaMalloc fail
+// or stall other work once it is running.  mm_prop_D_noalloc serves them: it
+// takes no handle and calls no cudaMalloc/cudaFree or allocating library
+// routine.  Its working memory -- the chirp and twiddle tables and the
+// column-pass intermediate -- lives in the file-scope array below, which
+// every GPU that loads this library holds (kNoAllocBytes) until the process
+// exits.  All calls share that one array and it keeps the last call's
+// contents, so calls that overlap on the GPU (two streams, two host threads)
+// race; callers must order them.  Nothing in it needs to start at zero: every
+// call rewrites the tables and the intermediate before reading them.
+static constexpr size_t kNoAllocBytes = 64ull << 20;  // 64 MiB per device
+static __device__ __align__(256) float2 g_noalloc_scratch[kNoAllocBytes / sizeof(float2)];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[64] = {nullptr};
+
+// Per-device set-up, done by the first call on each device (with that device
+// current): resolve the array's device address and upload the FFT constants.
+int noalloc_setup(float2** out) {
+    int dev = 0;
+    MM_CUDA(cudaGetDevice(&dev));
+    MM_REQUIRE(dev >= 0 && dev < 64, "mm_prop_D_noalloc: device %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            mm::set_error("mm_prop_D_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+            return MM_ECUDA;
+        }
+        MM_CUDA(mmfft::init_constants());
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = static_cast<float2*>(g_noalloc_ptr[dev]);
+    return MM_OK;
+}
+
+// Chirp and twiddle tables of one distance, computed on the device in FP64
+// exactly as chirp() / twiddles() do on the host for mm_prop_create.
+__global__ void k_noalloc_tables(float2* __restrict__ Kx, float2* __restrict__ Ky, float2* __restrict__ twx,
+                                 float2* __restrict__ twy, int n, int nz, double wavelength, double voxelsize,
+                                 double z) {
+    const int total = 2 * n + 2 * nz + 4 * n + 4 * nz;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        int i = t;
+        if (i < 2 * n + 2 * nz) {  // chirp along x then y
+            const bool along_x = i < 2 * n;
+            const int len = along_x ? 2 * n : 2 * nz;
+            const int k = along_x ? i : i - 2 * n;
+            const double val = 1.0 / (len * voxelsize);
+            const int kk = k < (len + 1) / 2 ? k : k - len;
+            const double f = (double)(float)(kk * val);
+            const double ph = fmod(M_PI * wavelength * z * f * f, 2.0 * M_PI);
+            const float2 w = make_float2((float)(cos(-ph) / len), (float)(sin(-ph) / len));
+            if (along_x) Kx[k] = w; else Ky[k] = w;
+            continue;
+        }
+        i -= 2 * n + 2 * nz;  // twiddles: x tables (2 * 2n) then y tables (2 * 2nz)
+        const bool along_x = i < 4 * n;
+        const int len = along_x ? 2 * n : 2 * nz;
+        int q = along_x ? i : i - 4 * n;
+        float2* tab = along_x ? twx : twy;
+        int r2 = 1;
+        while (r2 * r2 < len) r2 <<= 1;
+        if (r2 * r2 > len) r2 >>= 1;
+        const int r1 = len / r2;
+        int a, b;  // entry out[a*r2 + b] (q < len) or out[len + b*r1 + a]
+        if (q < len) { a = q / r2; b = q % r2; }
+        else { q -= len; b = q / r1; a = q % r1; q += len; }
+        const double ang = -2.0 * (double)(((long)a * b) % len) / len;
+        double s, c;
+        sincospi(ang, &s, &c);
+        tab[q] = make_float2((float)c, (float)s);
+    }
+}
+
+}  // namespace
+
+extern "C" int mm_prop_D_noalloc(int n, int nz, int ntheta, double wavelength, double voxelsize, double distance,
+                                 const void* psi, void* out, void* stream) {
+    MM_REQUIRE(psi != nullptr && out != nullptr, "mm_prop_D_noalloc: NULL array");
+    MM_REQUIRE(mm_is_pow2(2L * n) && 2 * n >= 4 && 2 * n <= 4096,
+               "mm_prop_D_noalloc: 2n=%d must be a power of two in [4, 4096]", 2 * n);
+    MM_REQUIRE(mm_is_pow2(2L * nz) && 2 * nz >= 4 && 2 * nz <= 4096,
+               "mm_prop_D_noalloc: 2nz=%d must be a power of two in [4, 4096]", 2 * nz);
+    MM_REQUIRE(ntheta >= 1 && voxelsize > 0, "mm_prop_D_noalloc: bad ntheta/voxelsize");
+    const size_t tables = (size_t)2 * n + 2 * nz + 4 * n + 4 * nz;
+    const size_t need = (tables + (size_t)ntheta * nz * n) * sizeof(float2);
+    MM_REQUIRE(need <= kNoAllocBytes,
+               "mm_prop_D_noalloc: ntheta*nz*n=%zu needs %zu bytes of scratch, more than the %zu-byte "
+               "static buffer (use mm_prop_D, or fewer angles per call)",
+               (size_t)ntheta * nz * n, need, kNoAllocBytes);
+    float2* base = nullptr;
+    MM_TRY(noalloc_setup(&base));
+    cudaStream_t st = (cudaStream_t)stream;
+    mm_prop h;  // view onto the static scratch; owns nothing
+    h.n = n;
+    h.nz = nz;
+    h.ntheta = ntheta;
+    h.ndist = 1;
+    h.Kx = base;
+    h.Ky = h.Kx + 2 * n;
+    h.twx = h.Ky + 2 * nz;
+    h.twy = h.twx + 4 * n;
+    h.mid = h.twy + 4 * nz;
+    k_noalloc_tables<<<(unsigned)((tables + 255) / 256), 256, 0, st>>>(h.Kx, h.Ky, h.twx, h.twy, n, nz, wavelength,
+                                                                      voxelsize, distance);
+    MM_LAUNCHED();
+    MM_TRY((dispatch_y<0, false>(&h, psi, ntheta, 0, 0.f, 0.f, st)));
+    return dispatch_x<0, false>(&h, out, ntheta, 0, st);
 }
