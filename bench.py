@@ -299,6 +299,45 @@ def run_ours(args, w, rank, world, local_rank):
     return line
 
 
+# ---------------------------------------------------------------- differentiable model
+MODEL = dict(n=512, nz=512, ntheta=1024, theta_max=np.pi, chunk=128)
+
+
+def run_model(args, local_rank):
+    """fwd+grad ms/iter of the L2 misfit of |D(exp(i(R delta + i R beta)))|^2 at
+    512^3 with 1024 angles, psi recomputed per 128-angle chunk: the fused
+    kernels against the same gradient composed from the unfused operators."""
+    import torch
+    from model_mosaic_b200.model import ForwardModel
+    from model_mosaic_b200.phantom import ellipsoid_volume_torch
+    w = WORKLOADS["production"]
+    n, nz, T = MODEL["n"], MODEL["nz"], MODEL["ntheta"]
+    dev = torch.device("cuda", local_rank)
+    theta = np.linspace(0, MODEL["theta_max"], T, endpoint=False).astype(np.float32)
+    m = ForwardModel(n, nz, theta, 1.24e-9 / w["energy_kev"], w["voxelsize"], w["distance"],
+                     angle_chunk=MODEL["chunk"])
+    delta = ellipsoid_volume_torch(n, nz, seed=0, device=dev)
+    data = m.forward(ellipsoid_volume_torch(n, nz, seed=1, device=dev))
+    st = torch.cuda.current_stream()
+    out = {}
+    for name, fn in (("fused", m.loss_and_grad), ("plain", m.plain_loss_and_grad)):
+        for _ in range(args.warmup):
+            fn(delta, data)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push(f"timed_model_{name}")
+        e0.record(st)
+        for _ in range(args.steps):
+            fn(delta, data)
+        e1.record(st)
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+        out[name + "_ms"] = round(e0.elapsed_time(e1) / args.steps, 3)
+    out["speedup_vs_plain"] = round(out["plain_ms"] / out["fused_ms"], 3)
+    out["config"] = f"{nz} slices of {n}^2, {T} angles on [0, pi), psi recomputed per {MODEL['chunk']}-angle chunk"
+    return out
+
+
 # ---------------------------------------------------------------- CPU (reference kernels on the host)
 def cpu_sample(w, slices=1, frames=32, cores=None):
     """Time the reference's kernels + restated glue on a bounded sample and
@@ -364,6 +403,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="production")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-rt", action="store_true", help="skip the adjoint (no scatter table)")
+    ap.add_argument("--no-model", action="store_true", help="skip the fwd+grad timing of the model")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -386,6 +426,8 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
     try:
         line = run_ours(args, w, rank, world, local_rank)
+        if args.workload == "production" and not args.no_model:
+            line["model_fwd_grad"] = run_model(args, local_rank)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             t, desc, kind, cores = cpu_sample(w)
             V = w["nz"] * w["n"] ** 2

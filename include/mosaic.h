@@ -114,13 +114,27 @@ int mm_prop_DT(mm_prop* h, const void* g, void* out, int ntheta, int j, void* st
 int mm_prop_intensity(mm_prop* h, const float* proj, float inv_norm, float inv_beta_ratio,
                       float* intensity, int ntheta, int j, void* stream);
 
+/* Differentiable forward model data = |D psi|^2, psi = exp(-p s/beta_r)(cos p s, sin p s),
+ * p = R delta (no reference counterpart: the reference composes R, psi, D and |.|^2 only
+ * across step2 -> disk -> step3 and has no adjoint of D).  With the L2 loss
+ * L = sum (|D psi|^2 - data)^2:
+ *   mm_prop_grad_forward: gu = 4 (|D psi|^2 - data) D psi (complex, (ntheta, nz, n)) and
+ *     per-block sums of (|D psi|^2 - data)^2 in partials[0 .. mm_prop_grad_partials());
+ *   mm_prop_grad_backward: gp = dL/dp = s Re(conj(D^H gu) (i - 1/beta_r) psi), float.
+ * dL/d delta is then mm_tomo_RT(gp).  inv_norm = s, inv_beta_ratio = 1/beta_r. */
+long mm_prop_grad_partials(mm_prop* h, int ntheta);
+int mm_prop_grad_forward(mm_prop* h, const float* proj, const float* data, float inv_norm,
+                         float inv_beta_ratio, void* gu, float* partials, int ntheta, int j, void* stream);
+int mm_prop_grad_backward(mm_prop* h, const void* gu, const float* proj, float inv_norm,
+                          float inv_beta_ratio, float* gp, int ntheta, int j, void* stream);
+
 /* Allocation-free Fresnel D for callers that cannot allocate device memory
  *   while they run (their GPU memory is reserved up front by their own pool
  *   allocator, so a cudaMalloc mid-run fails or stalls other work).  No
  *   counterpart in the reference.  Same operator and layouts as mm_prop_D for
  *   one distance, without a handle: the chirp/twiddle tables and the
  *   intermediate live in one static 64 MiB device array per GPU, so
- *   (ntheta*nz*n + 6*(n+nz)) * 8 bytes must fit in 64 MiB (MM_EINVAL
+ *   (ntheta*nz*n + 8*(n+nz)) * 8 bytes must fit in 64 MiB (MM_EINVAL
  *   otherwise).  The first call on each device resolves that array's address;
  *   make it before any stream capture.  Calls share the array: calls that
  *   overlap on the GPU race and must be ordered by the caller. */

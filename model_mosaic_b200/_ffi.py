@@ -54,7 +54,13 @@ def _declare(L):
     L.mm_tomo_get_timing.argtypes = [p, dp, llp, i, llp]
     L.mm_prop_set_timing.argtypes = [p, i]
     L.mm_prop_get_timing.argtypes = [p, dp, llp, i, llp]
-    for name in ("mm_tomo_set_timing", "mm_tomo_get_timing", "mm_prop_set_timing", "mm_prop_get_timing",
+    L.mm_prop_grad_partials.argtypes = [p, i]
+    L.mm_prop_grad_partials.restype = C.c_long
+    L.mm_prop_grad_forward.argtypes = [p, p, p, f, f, p, p, i, i, p]
+    L.mm_prop_grad_backward.argtypes = [p, p, p, f, f, p, i, i, p]
+    L.mm_prop_D_noalloc.argtypes = [i, i, i, d, d, d, p, p, p]
+    for name in ("mm_prop_grad_forward", "mm_prop_grad_backward", "mm_prop_D_noalloc",
+                 "mm_tomo_set_timing", "mm_tomo_get_timing", "mm_prop_set_timing", "mm_prop_get_timing",
                  "mm_tomo_create", "mm_tomo_destroy", "mm_tomo_R", "mm_tomo_RT", "mm_tomo_prepare_rt",
                  "mm_prop_create", "mm_prop_destroy", "mm_prop_D", "mm_prop_DT", "mm_prop_intensity"):
         getattr(L, name).restype = i

@@ -111,3 +111,220 @@ template <> struct Split<2048> { static constexpr int R1 = 64, R2 = 32; };
 template <> struct Split<4096> { static constexpr int R1 = 64, R2 = 64; };
 
 }  // namespace mmfft
+
+// ---------------------------------------------------------------------------
+// Stockham radix-16 FFT of one line of length L held in shared memory.
+//
+// G = L/16 threads cooperate on a line (t in [0, G)); each holds 16 complex
+// values per pass.  Pass p has span NS = 16^p and radix RP = 16 except the
+// last, RP = L / 16^(P-1).  In a pass every group j = t + G*q reads
+// x[j + i*L/RP] (i < RP), multiplies by W_{NS*RP}^(i*(j mod NS)), does an
+// RP-point register FFT and writes y[(j/NS)*NS*RP + (j mod NS) + i*NS]:
+// natural order in, natural order out, no bit reversal.  The first pass reads
+// through `ld(pos)` and the last writes through `st(pos, value)`, so a
+// transform can start from global memory and end in global memory; the
+// passes in between use `buf` through the addressing functor `ad(pos)`.
+// Twiddles: per pass p >= 1 a table tw + off_p with W_{NS*RP}^(i*k) at
+// [i*NS + k]; lanes with consecutive j read consecutive entries.
+namespace stockham {
+
+using mmfft::cmul;
+using mmfft::cmulc;
+using mmfft::ilog2;
+using mmfft::reg_fft;
+
+// Schedule of a length-L line: passes of radix 16 and one smaller radix
+// (L not a power of 16), the small one last (REV = false) or first (REV =
+// true).  The inverse half of a convolution uses the reversed schedule so
+// that its first pass owns exactly the elements the forward's last pass
+// produced (see conv()).
+template <int L, bool REV = false>
+struct Sched {
+    static constexpr int P = L <= 16 ? 1 : (ilog2<L>() + 3) / 4;   // passes
+    static constexpr int G = L >= 16 ? L / 16 : 1;                  // threads per line
+    static constexpr int V = L >= 16 ? 16 : L;                      // values per thread
+    static constexpr int small = L >> (4 * (P - 1));
+    static constexpr int radix(int p) { return REV ? (p == 0 ? small : 16) : (p < P - 1 ? 16 : small); }
+    static constexpr int span(int p) {
+        int s = 1;
+        for (int q = 0; q < p; ++q) s *= radix(q);
+        return s;
+    }
+    static constexpr int tw_off(int p) {  // start of pass p's table
+        int o = 0;
+        for (int q = 1; q < p; ++q) o += span(q) * radix(q);
+        return o;
+    }
+    static constexpr int tw_size() { return tw_off(P); }
+};
+
+// Host-side table for Sched<L, rev> (FP64 angles), Sched<L, rev>::tw_size()
+// entries: pass p >= 1, W_{NS*RP}^(i*k) at [off_p + i*NS + k].
+inline int host_twiddles(int L, bool rev, float2* out) {
+    int P = 1;
+    if (L > 16) {
+        int lg = 0;
+        while ((1 << lg) < L) ++lg;
+        P = (lg + 3) / 4;
+    }
+    const int small = L >> (4 * (P - 1));
+    auto radix = [&](int p) { return rev ? (p == 0 ? small : 16) : (p < P - 1 ? 16 : small); };
+    int o = 0, ns = radix(0);
+    for (int p = 1; p < P; ++p) {
+        const int rp = radix(p);
+        for (int i = 0; i < rp; ++i)
+            for (int k = 0; k < ns; ++k) {
+                const double a = -2.0 * 3.14159265358979323846 * (double)((long)i * k % (ns * rp)) / (ns * rp);
+                out[o + i * ns + k] = make_float2((float)cos(a), (float)sin(a));
+            }
+        o += ns * rp;
+        ns *= rp;
+    }
+    return o;
+}
+
+// Registers of one thread in pass PASS: groups j = t + G*q, element i of
+// group j at line position j + i*NG.
+template <int L, bool REV, int PASS>
+struct PassShape {
+    using S = Sched<L, REV>;
+    static constexpr int RP = S::radix(PASS);
+    static constexpr int NS = S::span(PASS);
+    static constexpr int NG = L / RP;
+    static constexpr int Q = NG / S::G;
+    static_assert(Q * RP == S::V, "16 values per thread");
+};
+
+template <int L, bool REV, int PASS, bool INV, class Src>
+__device__ __forceinline__ void pass_load(float2 (&x)[PassShape<L, REV, PASS>::Q][PassShape<L, REV, PASS>::RP],
+                                          const Src& src, int t, const float2* __restrict__ tw) {
+    using Sh = PassShape<L, REV, PASS>;
+    using S = Sched<L, REV>;
+#pragma unroll
+    for (int q = 0; q < Sh::Q; ++q) {
+        const int j = t + S::G * q;
+#pragma unroll
+        for (int i = 0; i < Sh::RP; ++i) x[q][i] = src(j + i * Sh::NG);
+        if (Sh::NS > 1) {
+            const int k = j & (Sh::NS - 1);
+            const float2* tp = tw + S::tw_off(PASS);
+#pragma unroll
+            for (int i = 1; i < Sh::RP; ++i) {
+                const float2 w = __ldg(tp + i * Sh::NS + k);
+                x[q][i] = INV ? cmulc(x[q][i], w) : cmul(x[q][i], w);
+            }
+        }
+        reg_fft<Sh::RP, INV>(x[q]);
+    }
+}
+
+template <int L, bool REV, int PASS, class Dst>
+__device__ __forceinline__ void pass_store(float2 (&x)[PassShape<L, REV, PASS>::Q][PassShape<L, REV, PASS>::RP],
+                                           const Dst& dst, int t) {
+    using Sh = PassShape<L, REV, PASS>;
+    using S = Sched<L, REV>;
+#pragma unroll
+    for (int q = 0; q < Sh::Q; ++q) {
+        const int j = t + S::G * q;
+        const int k = j & (Sh::NS - 1);
+        const int base = (j / Sh::NS) * Sh::NS * Sh::RP + k;
+#pragma unroll
+        for (int i = 0; i < Sh::RP; ++i) dst(base + i * Sh::NS, x[q][i]);
+    }
+}
+
+// Passes FIRST..LAST of a transform through shared memory; pass 0 reads
+// through `ld`, pass P-1 writes through `st`, every other access is buf.
+template <int L, bool REV, bool INV, int PASS, int LAST, class Ld, class St, class Ad>
+__device__ __forceinline__ void run(float2* __restrict__ buf, const Ad& ad, const Ld& ld, const St& st, int t,
+                                   const float2* __restrict__ tw) {
+    using Sh = PassShape<L, REV, PASS>;
+    using S = Sched<L, REV>;
+    float2 x[Sh::Q][Sh::RP];
+    auto from_buf = [&](int pos) -> float2 { return buf[ad(pos)]; };
+    if constexpr (PASS == 0) pass_load<L, REV, PASS, INV>(x, ld, t, tw);
+    else pass_load<L, REV, PASS, INV>(x, from_buf, t, tw);
+    __syncthreads();  // everyone has read this pass's input
+    if constexpr (PASS == S::P - 1) {
+        pass_store<L, REV, PASS>(x, st, t);
+    } else {
+        auto to_buf = [&](int pos, float2 v) { buf[ad(pos)] = v; };
+        pass_store<L, REV, PASS>(x, to_buf, t);
+        __syncthreads();
+    }
+    if constexpr (PASS < LAST) run<L, REV, INV, PASS + 1, LAST>(buf, ad, ld, st, t, tw);
+}
+
+// One transform: natural order in (`ld`) and out (`st`).  Callers
+// synchronise before reusing `buf` after it returns.  tw: Sched<L, false>.
+template <int L, bool INV, class Ld, class St, class Ad>
+__device__ __forceinline__ void fft(float2* __restrict__ buf, const Ad& ad, const Ld& ld, const St& st, int t,
+                                    const float2* __restrict__ tw) {
+    run<L, false, INV, 0, Sched<L>::P - 1>(buf, ad, ld, st, t, tw);
+}
+
+// Circular convolution y = IFFT(mul(k) * FFT(x)) (both unnormalised): the
+// forward's last pass, the pointwise multiply and the inverse's first pass
+// (reversed schedule) run on the same registers.  twf: Sched<L, false>
+// table; twi: Sched<L, true> table.  `mul(pos, X)` returns the product for
+// spectral index pos.
+template <int L, class Ld, class Mul, class St, class Ad>
+__device__ __forceinline__ void conv(float2* __restrict__ buf, const Ad& ad, const Ld& ld, const Mul& mul,
+                                     const St& st, int t, const float2* __restrict__ twf,
+                                     const float2* __restrict__ twi) {
+    using F = Sched<L, false>;
+    using I = Sched<L, true>;
+    constexpr int P = F::P;
+    if constexpr (P == 1) {
+        using Sh = PassShape<L, false, 0>;
+        float2 x[Sh::Q][Sh::RP];
+        pass_load<L, false, 0, false>(x, ld, t, twf);
+#pragma unroll
+        for (int q = 0; q < Sh::Q; ++q) {
+#pragma unroll
+            for (int i = 0; i < Sh::RP; ++i) x[q][i] = mul((t + F::G * q) + i * Sh::NG, x[q][i]);
+            reg_fft<Sh::RP, true>(x[q]);
+        }
+        __syncthreads();
+        pass_store<L, false, 0>(x, st, t);
+    } else {
+        auto to_buf = [&](int pos, float2 v) { buf[ad(pos)] = v; };
+        auto from_buf = [&](int pos) -> float2 { return buf[ad(pos)]; };
+        run<L, false, false, 0, P - 2>(buf, ad, ld, to_buf, t, twf);
+        using Sf = PassShape<L, false, P - 1>;
+        using Si = PassShape<L, true, 0>;
+        static_assert(Sf::RP == Si::RP && Sf::NG == Si::NG && Sf::Q == Si::Q, "fused pass shapes");
+        float2 x[Sf::Q][Sf::RP];
+        pass_load<L, false, P - 1, false>(x, from_buf, t, twf);
+#pragma unroll
+        for (int q = 0; q < Sf::Q; ++q) {
+            const int j = t + F::G * q;  // forward output k = j + i*NG; inverse input j + i*NG
+#pragma unroll
+            for (int i = 0; i < Sf::RP; ++i) x[q][i] = mul(j + i * Sf::NG, x[q][i]);
+            reg_fft<Sf::RP, true>(x[q]);
+        }
+        __syncthreads();
+        pass_store<L, true, 0>(x, to_buf, t);
+        __syncthreads();
+        run<L, true, true, 1, P - 1>(buf, ad, ld, st, t, twi);
+    }
+}
+
+// Shared-memory addressing: a row line with one pad slot per 16 entries, or
+// column lines interleaved with lanes running over CW columns.
+struct RowAddr {
+    int base;
+    __device__ __forceinline__ int operator()(int pos) const { return base + pos + (pos >> 4); }
+};
+// With fewer than 16 columns one pad row per 16 keeps the radix-16 pass
+// writes (position stride 16) free of bank conflicts.
+template <int CW>
+struct ColAddr {
+    int col;
+    __device__ __forceinline__ int operator()(int pos) const {
+        return CW >= 16 ? pos * CW + col : (pos + (pos >> 4)) * CW + col;
+    }
+    static constexpr int rows(int L) { return CW >= 16 ? L : L + L / 16; }
+};
+
+}  // namespace stockham

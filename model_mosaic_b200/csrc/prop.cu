@@ -32,10 +32,10 @@ struct mm_prop {
     int n = 0, nz = 0, ntheta = 0, ndist = 0;
     float2* Kx = nullptr;   // (ndist, 2n)
     float2* Ky = nullptr;   // (ndist, 2nz)
-    // inter-step twiddles W_L^(k1*n2) of L = R1*R2 as two tables laid out so
-    // that the lanes of a warp read consecutive entries: A[k1][n2], B[n2][k1]
-    float2* twx = nullptr;  // (2 * 2n)  x: A then B
-    float2* twy = nullptr;  // (2 * 2nz) y: A then B
+    // Stockham pass twiddles of the 2n- and 2nz-point lines (fft_smem.cuh),
+    // each in a 3L-entry slot (forward schedule, then reversed at 3L/2)
+    float2* twx = nullptr;  // (3 * 2n)
+    float2* twy = nullptr;  // (3 * 2nz)
     float2* mid = nullptr;  // (ntheta, nz, n)
     size_t ws_bytes = 0;
     mm::StageTimer tm;
@@ -55,24 +55,26 @@ __device__ __forceinline__ int mirror_partner(int r, int len) {
 }
 
 // ---------------------------------------------------------------- y-pass
-// IN: 0 complex psi, 1 real projection (psi built on load).  Block (CW, R2):
-// lanes run over CW adjacent columns, threadIdx.y over the R2 sub-sequences.
+// IN: 0 complex psi, 1 real projection (psi built on load).  Block (CW, G):
+// lanes run over CW adjacent columns, threadIdx.y over the G = 2nz/16
+// threads of each column's Stockham transform (fft_smem.cuh).
 template <int L, int CW, int IN, bool ADJ>
-__global__ void __launch_bounds__(CW * Split<L>::R2) k_ypass(const void* __restrict__ src, float2* __restrict__ dst,
-                                                            const float2* __restrict__ Ky,
-                                                            const float2* __restrict__ tw, int n, int nz,
-                                                            float s, float ib) {
-    constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2;
-    extern __shared__ float2 sm[];  // [R1][R2][CW]
+__global__ void __launch_bounds__(CW * stockham::Sched<L>::G, 1024 / (CW * stockham::Sched<L>::G)) k_ypass(const void* __restrict__ src,
+                                                                       float2* __restrict__ dst,
+                                                                       const float2* __restrict__ Ky,
+                                                                       const float2* __restrict__ tw, int n, int nz,
+                                                                       float s, float ib) {
+    using S = stockham::Sched<L>;
+    extern __shared__ float2 sm[];  // buf [L][CW], then staged rows [nz][CW]
+    float2* buf = sm;
+    float2* stg = sm + L * CW;
     const int c = threadIdx.x, g = threadIdx.y;
     const int x = blockIdx.x * CW + c;
     const bool live = x < n;
     const long plane = (long)blockIdx.y * nz * n;
-    const float2* twA = tw;          // [R1][R2]
-    const float2* twB = tw + L;      // [R2][R1]
     // stage the nz source rows of this column block once (psi built here);
     // the mirror padding then reads each of them twice from shared memory
-    for (int r = g; r < nz; r += R2) {
+    for (int r = g; r < nz; r += S::G) {
         float2 a = make_float2(0.f, 0.f);
         if (live) {
             const long off = plane + (long)r * n + x;
@@ -86,150 +88,120 @@ __global__ void __launch_bounds__(CW * Split<L>::R2) k_ypass(const void* __restr
                 a = make_float2(at * cs, at * sn);
             }
         }
-        sm[r * CW + c] = a;
+        stg[r * CW + c] = a;
     }
     __syncthreads();
-    float2 v[R1];
-#pragma unroll
-    for (int n1 = 0; n1 < R1; ++n1) {
-        const int idx = R2 * n1 + g;
-        int r;
-        bool zero = false;
-        if (!ADJ) {
-            r = mirror_src(idx, nz);
-        } else {
-            r = idx - nz / 2;
-            zero = r < 0 || r >= nz;
-        }
-        v[n1] = zero ? make_float2(0.f, 0.f) : sm[r * CW + c];
-    }
-    __syncthreads();
-    reg_fft<R1, false>(v);
-#pragma unroll
-    for (int k1 = 1; k1 < R1; ++k1)
-        if (g) v[k1] = cmul(v[k1], __ldg(twA + k1 * R2 + g));
-#pragma unroll
-    for (int k1 = 0; k1 < R1; ++k1) sm[(k1 * R2 + g) * CW + c] = v[k1];
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < R1 / R2; ++i) {
-        const int k1 = g + R2 * i;
-        float2 u[R2];
-#pragma unroll
-        for (int n2 = 0; n2 < R2; ++n2) u[n2] = sm[(k1 * R2 + n2) * CW + c];
-        reg_fft<R2, false>(u);
-#pragma unroll
-        for (int k2 = 0; k2 < R2; ++k2) {
-            const float2 K = __ldg(Ky + k1 + R1 * k2);
-            u[k2] = ADJ ? cmulc(u[k2], K) : cmul(u[k2], K);
-        }
-        reg_fft<R2, true>(u);
-#pragma unroll
-        for (int m2 = 1; m2 < R2; ++m2)
-            if (k1) u[m2] = cmulc(u[m2], __ldg(twB + m2 * R1 + k1));
-#pragma unroll
-        for (int m2 = 0; m2 < R2; ++m2) sm[(k1 * R2 + m2) * CW + c] = u[m2];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k1 = 0; k1 < R1; ++k1) v[k1] = sm[(k1 * R2 + g) * CW + c];
-    reg_fft<R1, true>(v);
+    const stockham::ColAddr<CW> ad{c};
+    auto ld_in = [&](int pos) -> float2 {
+        if (!ADJ) return stg[mirror_src(pos, nz) * CW + c];
+        const int r = pos - nz / 2;
+        return (r >= 0 && r < nz) ? stg[r * CW + c] : make_float2(0.f, 0.f);
+    };
+    auto mul = [&](int pos, float2 v) -> float2 {
+        const float2 K = __ldg(Ky + pos);
+        return ADJ ? cmulc(v, K) : cmul(v, K);
+    };
+    const float2* twf = tw;
+    const float2* twi = tw + 3 * L / 2;
     if (!ADJ) {
-#pragma unroll
-        for (int m1 = 0; m1 < R1; ++m1) {
-            const int r = g + R2 * m1 - nz / 2;
-            if (live && r >= 0 && r < nz) dst[plane + (long)r * n + x] = v[m1];
-        }
+        auto st_out = [&](int pos, float2 v) {
+            const int r = pos - nz / 2;
+            if (live && r >= 0 && r < nz) dst[plane + (long)r * n + x] = v;
+        };
+        stockham::conv<L>(buf, ad, ld_in, mul, st_out, g, twf, twi);
     } else {
+        auto st_b = [&](int pos, float2 v) { buf[pos * CW + c] = v; };
+        stockham::conv<L>(buf, ad, ld_in, mul, st_b, g, twf, twi);
         __syncthreads();
-#pragma unroll
-        for (int m1 = 0; m1 < R1; ++m1) sm[(g + R2 * m1) * CW + c] = v[m1];
-        __syncthreads();
-        for (int r = g; r < nz; r += R2) {
-            const float2 a = sm[(r + nz / 2) * CW + c], b = sm[mirror_partner(r, nz) * CW + c];
+        for (int r = g; r < nz; r += S::G) {
+            const float2 a = buf[(r + nz / 2) * CW + c], b = buf[mirror_partner(r, nz) * CW + c];
             if (live) dst[plane + (long)r * n + x] = make_float2(a.x + b.x, a.y + b.y);
         }
     }
 }
 
 // ---------------------------------------------------------------- x-pass
-// OUT: 0 complex, 1 |.|^2 float.  Block (R2, RPB): R2 threads per row.
+// OUT: 0 complex, 1 |.|^2 float, 2 (forward, gradient of the L2 loss):
+// g = 4 (|u|^2 - d) u with d = aux, plus per-block sums of (|u|^2 - d)^2
+// in partials[blockIdx.x]; 3 (adjoint, chain through psi): dL/dp =
+// s Re(conj(g) (i - ib) psi(p)) with p = aux, psi(p) = exp(-p s ib)(cos p s,
+// sin p s), written as float.  Block (G, RPB): G = 2n/16 threads per row.
 template <int L, int RPB, int OUT, bool ADJ>
-__global__ void __launch_bounds__(RPB * Split<L>::R2) k_xpass(const float2* __restrict__ src, void* __restrict__ dst,
-                                                             const float2* __restrict__ Kx,
-                                                             const float2* __restrict__ tw, int n, long rows) {
-    constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2, P = R2 + 1;
-    extern __shared__ float2 sm[];  // [RPB][R1][R2 + 1]
+__global__ void __launch_bounds__(RPB * stockham::Sched<L>::G, 512 / (RPB * stockham::Sched<L>::G)) k_xpass(const float2* __restrict__ src,
+                                                                        void* __restrict__ dst,
+                                                                        const float2* __restrict__ Kx,
+                                                                        const float2* __restrict__ tw, int n,
+                                                                        long rows, const float* __restrict__ aux,
+                                                                        float* __restrict__ partials, float s,
+                                                                        float ib) {
+    extern __shared__ float2 sm[];  // [RPB][L + L/16]
+    constexpr int LP = L + L / 16;
     const int g = threadIdx.x, rr = threadIdx.y;
     const long row = (long)blockIdx.x * RPB + rr;
     const bool live = row < rows;
-    float2* S = sm + rr * R1 * P;
+    const stockham::RowAddr ad{rr * LP};
+    float2* buf = sm;
     const float2* in = src + row * n;
-    const float2* twA = tw;          // [R1][R2]
-    const float2* twB = tw + L;      // [R2][R1]
-    float2 v[R1];
-#pragma unroll
-    for (int n1 = 0; n1 < R1; ++n1) {
-        const int idx = R2 * n1 + g;
-        int col;
-        bool zero = false;
-        if (!ADJ) {
-            col = mirror_src(idx, n);
-        } else {
-            col = idx - n / 2;
-            zero = col < 0 || col >= n;
-        }
-        v[n1] = (live && !zero) ? __ldg(in + col) : make_float2(0.f, 0.f);
-    }
-    reg_fft<R1, false>(v);
-#pragma unroll
-    for (int k1 = 1; k1 < R1; ++k1)
-        if (g) v[k1] = cmul(v[k1], __ldg(twA + k1 * R2 + g));
-#pragma unroll
-    for (int k1 = 0; k1 < R1; ++k1) S[k1 * P + g] = v[k1];
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < R1 / R2; ++i) {
-        const int k1 = g + R2 * i;
-        float2 u[R2];
-#pragma unroll
-        for (int n2 = 0; n2 < R2; ++n2) u[n2] = S[k1 * P + n2];
-        reg_fft<R2, false>(u);
-#pragma unroll
-        for (int k2 = 0; k2 < R2; ++k2) {
-            const float2 K = __ldg(Kx + k1 + R1 * k2);
-            u[k2] = ADJ ? cmulc(u[k2], K) : cmul(u[k2], K);
-        }
-        reg_fft<R2, true>(u);
-#pragma unroll
-        for (int m2 = 1; m2 < R2; ++m2)
-            if (k1) u[m2] = cmulc(u[m2], __ldg(twB + m2 * R1 + k1));
-#pragma unroll
-        for (int m2 = 0; m2 < R2; ++m2) S[k1 * P + m2] = u[m2];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k1 = 0; k1 < R1; ++k1) v[k1] = S[k1 * P + g];
-    reg_fft<R1, true>(v);
+    auto ld_in = [&](int pos) -> float2 {
+        int col = ADJ ? pos - n / 2 : mirror_src(pos, n);
+        if (ADJ && (col < 0 || col >= n)) return make_float2(0.f, 0.f);
+        return live ? __ldg(in + col) : make_float2(0.f, 0.f);
+    };
+    auto mul = [&](int pos, float2 v) -> float2 {
+        const float2 K = __ldg(Kx + pos);
+        return ADJ ? cmulc(v, K) : cmul(v, K);
+    };
+    const float2* twf = tw;
+    const float2* twi = tw + 3 * L / 2;
     if (!ADJ) {
-#pragma unroll
-        for (int m1 = 0; m1 < R1; ++m1) {
-            const int c = g + R2 * m1 - n / 2;
+        float lsum = 0.f;
+        auto st_out = [&](int pos, float2 v) {
+            const int c = pos - n / 2;
             if (live && c >= 0 && c < n) {
-                if (OUT == 0)
-                    static_cast<float2*>(dst)[row * n + c] = v[m1];
-                else
-                    static_cast<float*>(dst)[row * n + c] = v[m1].x * v[m1].x + v[m1].y * v[m1].y;
+                if (OUT == 0) {
+                    static_cast<float2*>(dst)[row * n + c] = v;
+                } else if (OUT == 1) {
+                    static_cast<float*>(dst)[row * n + c] = v.x * v.x + v.y * v.y;
+                } else {
+                    const float r = v.x * v.x + v.y * v.y - __ldg(aux + row * n + c);
+                    lsum = fmaf(r, r, lsum);
+                    static_cast<float2*>(dst)[row * n + c] = make_float2(4.f * r * v.x, 4.f * r * v.y);
+                }
+            }
+        };
+        stockham::conv<L>(buf, ad, ld_in, mul, st_out, g, twf, twi);
+        if (OUT == 2) {  // deterministic block sum of the squared residuals
+            __syncthreads();
+            float* red = reinterpret_cast<float*>(sm);
+            for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+            const int tid = rr * blockDim.x + g, nw = (blockDim.x * blockDim.y + 31) / 32;
+            if ((tid & 31) == 0) red[tid >> 5] = lsum;
+            __syncthreads();
+            if (tid == 0) {
+                float t = 0.f;
+                for (int w = 0; w < nw; ++w) t += red[w];
+                partials[blockIdx.x] = t;
             }
         }
     } else {
+        auto st_b = [&](int pos, float2 v) { buf[ad(pos)] = v; };
+        stockham::conv<L>(buf, ad, ld_in, mul, st_b, g, twf, twi);
         __syncthreads();
-#pragma unroll
-        for (int m1 = 0; m1 < R1; ++m1) S[g + R2 * m1] = v[m1];   // L <= R1 * P
-        __syncthreads();
-        for (int c = g; c < n; c += R2) {
-            const float2 a = S[c + n / 2], b = S[mirror_partner(c, n)];
-            if (live) static_cast<float2*>(dst)[row * n + c] = make_float2(a.x + b.x, a.y + b.y);
+        for (int c = g; c < n; c += stockham::Sched<L>::G) {
+            const float2 a = buf[ad(c + n / 2)], b = buf[ad(mirror_partner(c, n))];
+            if (!live) continue;
+            const float2 gv = make_float2(a.x + b.x, a.y + b.y);
+            if (OUT == 3) {
+                const float ph = __ldg(aux + row * n + c) * s;
+                const float at = expf(-ph * ib);
+                float sn, cs;
+                sincosf(ph, &sn, &cs);
+                const float px = at * cs, py = at * sn;              // psi
+                const float wx = -ib * px - py, wy = px - ib * py;   // (i - ib) psi
+                static_cast<float*>(dst)[row * n + c] = s * (gv.x * wx + gv.y * wy);
+            } else {
+                static_cast<float2*>(dst)[row * n + c] = gv;
+            }
         }
     }
 }
@@ -237,13 +209,13 @@ __global__ void __launch_bounds__(RPB * Split<L>::R2) k_xpass(const float2* __re
 // ---------------------------------------------------------------- launch
 template <int L, int IN, bool ADJ>
 int launch_y(mm_prop* h, const void* src, int ntheta, int j, float s, float ib, cudaStream_t st) {
-    constexpr int R2 = Split<L>::R2;
-    constexpr int CW0 = 256 / R2;
+    constexpr int G = stockham::Sched<L>::G;
+    constexpr int CW0 = 256 / G;
     constexpr int CW = CW0 < 4 ? 4 : (CW0 > 32 ? 32 : CW0);
-    const size_t smem = (size_t)L * CW * sizeof(float2);
+    const size_t smem = (size_t)(L * CW + (L / 2) * CW) * sizeof(float2);
     auto kern = k_ypass<L, CW, IN, ADJ>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 block(CW, R2), grid((h->n + CW - 1) / CW, ntheta);
+    dim3 block(CW, G), grid((h->n + CW - 1) / CW, ntheta);
     h->tm.begin(0, st);
     kern<<<grid, block, smem, st>>>(src, h->mid, h->Ky + (size_t)j * 2 * h->nz, h->twy, h->n, h->nz, s, ib);
     MM_LAUNCHED();
@@ -252,16 +224,18 @@ int launch_y(mm_prop* h, const void* src, int ntheta, int j, float s, float ib, 
 }
 
 template <int L, int OUT, bool ADJ>
-int launch_x(mm_prop* h, void* dst, int ntheta, int j, cudaStream_t st) {
-    constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2;
-    constexpr int RPB = R2 >= 128 ? 1 : 128 / R2;
-    const size_t smem = (size_t)RPB * R1 * (R2 + 1) * sizeof(float2);
+int launch_x(mm_prop* h, void* dst, int ntheta, int j, cudaStream_t st, const float* aux = nullptr,
+             float* partials = nullptr, float s = 0.f, float ib = 0.f) {
+    constexpr int G = stockham::Sched<L>::G;
+    constexpr int RPB = G >= 256 ? 1 : 256 / G;
+    const size_t smem = (size_t)RPB * (L + L / 16) * sizeof(float2);
     auto kern = k_xpass<L, RPB, OUT, ADJ>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long rows = (long)ntheta * h->nz;
-    dim3 block(R2, RPB), grid((unsigned)((rows + RPB - 1) / RPB));
+    dim3 block(G, RPB), grid((unsigned)((rows + RPB - 1) / RPB));
     h->tm.begin(1, st);
-    kern<<<grid, block, smem, st>>>(h->mid, dst, h->Kx + (size_t)j * 2 * h->n, h->twx, h->n, rows);
+    kern<<<grid, block, smem, st>>>(h->mid, dst, h->Kx + (size_t)j * 2 * h->n, h->twx, h->n, rows, aux, partials,
+                                    s, ib);
     MM_LAUNCHED();
     h->tm.end(st, 1);
     return MM_OK;
@@ -286,19 +260,20 @@ int dispatch_y(mm_prop* h, const void* src, int ntheta, int j, float s, float ib
 }
 
 template <int OUT, bool ADJ>
-int dispatch_x(mm_prop* h, void* dst, int ntheta, int j, cudaStream_t st) {
+int dispatch_x(mm_prop* h, void* dst, int ntheta, int j, cudaStream_t st, const float* aux = nullptr,
+               float* partials = nullptr, float s = 0.f, float ib = 0.f) {
     switch (2 * h->n) {
-        case 4: return launch_x<4, OUT, ADJ>(h, dst, ntheta, j, st);
-        case 8: return launch_x<8, OUT, ADJ>(h, dst, ntheta, j, st);
-        case 16: return launch_x<16, OUT, ADJ>(h, dst, ntheta, j, st);
-        case 32: return launch_x<32, OUT, ADJ>(h, dst, ntheta, j, st);
-        case 64: return launch_x<64, OUT, ADJ>(h, dst, ntheta, j, st);
-        case 128: return launch_x<128, OUT, ADJ>(h, dst, ntheta, j, st);
-        case 256: return launch_x<256, OUT, ADJ>(h, dst, ntheta, j, st);
-        case 512: return launch_x<512, OUT, ADJ>(h, dst, ntheta, j, st);
-        case 1024: return launch_x<1024, OUT, ADJ>(h, dst, ntheta, j, st);
-        case 2048: return launch_x<2048, OUT, ADJ>(h, dst, ntheta, j, st);
-        case 4096: return launch_x<4096, OUT, ADJ>(h, dst, ntheta, j, st);
+        case 4: return launch_x<4, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
+        case 8: return launch_x<8, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
+        case 16: return launch_x<16, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
+        case 32: return launch_x<32, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
+        case 64: return launch_x<64, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
+        case 128: return launch_x<128, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
+        case 256: return launch_x<256, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
+        case 512: return launch_x<512, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
+        case 1024: return launch_x<1024, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
+        case 2048: return launch_x<2048, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
+        case 4096: return launch_x<4096, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
     }
     MM_REQUIRE(false, "unsupported 2*n=%d", 2 * h->n);
 }
@@ -331,21 +306,12 @@ void chirp(std::vector<float2>& out, int len, double voxelsize, double wavelengt
     }
 }
 
-// Two layouts of W_len^(i*j), i < R1, j < R2 (R1 >= R2 as in mmfft::Split):
-// out[i*R2 + j] and out[len + j*R1 + i].
+// Stockham twiddle tables of a length-len line (fft_smem.cuh) in a 3*len
+// slot: the forward schedule's at 0, the reversed schedule's at 3*len/2.
 void twiddles(std::vector<float2>& out, int len) {
-    int r2 = 1;
-    while (r2 * r2 < len) r2 <<= 1;
-    if (r2 * r2 > len) r2 >>= 1;
-    const int r1 = len / r2;
-    out.assign(2 * (size_t)len, make_float2(0.f, 0.f));
-    for (int i = 0; i < r1; ++i)
-        for (int j = 0; j < r2; ++j) {
-            const double a = -2.0 * M_PI * (double)((long)i * j % len) / len;
-            const float2 w = make_float2((float)cos(a), (float)sin(a));
-            out[(size_t)i * r2 + j] = w;
-            out[len + (size_t)j * r1 + i] = w;
-        }
+    out.assign(3 * (size_t)len, make_float2(0.f, 0.f));
+    stockham::host_twiddles(len, false, out.data());
+    stockham::host_twiddles(len, true, out.data() + 3 * len / 2);
 }
 
 }  // namespace
@@ -500,7 +466,7 @@ int noalloc_setup(float2** out) {
 __global__ void k_noalloc_tables(float2* __restrict__ Kx, float2* __restrict__ Ky, float2* __restrict__ twx,
                                  float2* __restrict__ twy, int n, int nz, double wavelength, double voxelsize,
                                  double z) {
-    const int total = 2 * n + 2 * nz + 4 * n + 4 * nz;
+    const int total = 2 * n + 2 * nz + 6 * n + 6 * nz;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         int i = t;
         if (i < 2 * n + 2 * nz) {  // chirp along x then y
@@ -515,22 +481,36 @@ __global__ void k_noalloc_tables(float2* __restrict__ Kx, float2* __restrict__ K
             if (along_x) Kx[k] = w; else Ky[k] = w;
             continue;
         }
-        i -= 2 * n + 2 * nz;  // twiddles: x tables (2 * 2n) then y tables (2 * 2nz)
-        const bool along_x = i < 4 * n;
+        i -= 2 * n + 2 * nz;  // twiddles: x slot (3 * 2n) then y slot (3 * 2nz)
+        const bool along_x = i < 6 * n;
         const int len = along_x ? 2 * n : 2 * nz;
-        int q = along_x ? i : i - 4 * n;
+        int q = along_x ? i : i - 6 * n;
         float2* tab = along_x ? twx : twy;
-        int r2 = 1;
-        while (r2 * r2 < len) r2 <<= 1;
-        if (r2 * r2 > len) r2 >>= 1;
-        const int r1 = len / r2;
-        int a, b;  // entry out[a*r2 + b] (q < len) or out[len + b*r1 + a]
-        if (q < len) { a = q / r2; b = q % r2; }
-        else { q -= len; b = q / r1; a = q % r1; q += len; }
-        const double ang = -2.0 * (double)(((long)a * b) % len) / len;
-        double s, c;
-        sincospi(ang, &s, &c);
-        tab[q] = make_float2((float)c, (float)s);
+        const int slot_q = q;
+        const bool rev = q >= 3 * len / 2;
+        if (rev) q -= 3 * len / 2;
+        // entry q of stockham::host_twiddles(len, rev, .)
+        int P = 1;
+        if (len > 16) {
+            int lg = 0;
+            while ((1 << lg) < len) ++lg;
+            P = (lg + 3) / 4;
+        }
+        const int small = len >> (4 * (P - 1));
+        int o = 0, ns = rev ? small : (P > 1 ? 16 : small);
+        float2 w = make_float2(0.f, 0.f);
+        for (int p = 1; p < P; ++p) {
+            const int rp = rev ? 16 : (p < P - 1 ? 16 : small);
+            if (q >= o && q < o + ns * rp) {
+                const int ii = (q - o) / ns, k = (q - o) % ns;
+                double sv, cv;
+                sincospi(-2.0 * (double)(((long)ii * k) % (ns * rp)) / (ns * rp), &sv, &cv);
+                w = make_float2((float)cv, (float)sv);
+            }
+            o += ns * rp;
+            ns *= rp;
+        }
+        tab[slot_q] = w;
     }
 }
 
@@ -544,7 +524,7 @@ extern "C" int mm_prop_D_noalloc(int n, int nz, int ntheta, double wavelength, d
     MM_REQUIRE(mm_is_pow2(2L * nz) && 2 * nz >= 4 && 2 * nz <= 4096,
                "mm_prop_D_noalloc: 2nz=%d must be a power of two in [4, 4096]", 2 * nz);
     MM_REQUIRE(ntheta >= 1 && voxelsize > 0, "mm_prop_D_noalloc: bad ntheta/voxelsize");
-    const size_t tables = (size_t)2 * n + 2 * nz + 4 * n + 4 * nz;
+    const size_t tables = (size_t)8 * n + 8 * nz;
     const size_t need = (tables + (size_t)ntheta * nz * n) * sizeof(float2);
     MM_REQUIRE(need <= kNoAllocBytes,
                "mm_prop_D_noalloc: ntheta*nz*n=%zu needs %zu bytes of scratch, more than the %zu-byte "
@@ -561,11 +541,37 @@ extern "C" int mm_prop_D_noalloc(int n, int nz, int ntheta, double wavelength, d
     h.Kx = base;
     h.Ky = h.Kx + 2 * n;
     h.twx = h.Ky + 2 * nz;
-    h.twy = h.twx + 4 * n;
-    h.mid = h.twy + 4 * nz;
+    h.twy = h.twx + 6 * n;
+    h.mid = h.twy + 6 * nz;
     k_noalloc_tables<<<(unsigned)((tables + 255) / 256), 256, 0, st>>>(h.Kx, h.Ky, h.twx, h.twy, n, nz, wavelength,
                                                                       voxelsize, distance);
     MM_LAUNCHED();
     MM_TRY((dispatch_y<0, false>(&h, psi, ntheta, 0, 0.f, 0.f, st)));
     return dispatch_x<0, false>(&h, out, ntheta, 0, st);
+}
+
+extern "C" long mm_prop_grad_partials(mm_prop* h, int ntheta) {
+    if (!h || ntheta < 1) return 0;
+    const int G = (2 * h->n) >= 16 ? (2 * h->n) / 16 : 1;
+    const int rpb = G >= 256 ? 1 : 256 / G;
+    return ((long)ntheta * h->nz + rpb - 1) / rpb;
+}
+
+extern "C" int mm_prop_grad_forward(mm_prop* h, const float* proj, const float* data, float inv_norm,
+                                    float inv_beta_ratio, void* gu, float* partials, int ntheta, int j,
+                                    void* stream) {
+    MM_TRY(check_call(h, proj, gu, ntheta, j, "mm_prop_grad_forward"));
+    MM_REQUIRE(data != nullptr && partials != nullptr, "mm_prop_grad_forward: NULL data/partials");
+    cudaStream_t st = (cudaStream_t)stream;
+    MM_TRY((dispatch_y<1, false>(h, proj, ntheta, j, inv_norm, inv_beta_ratio, st)));
+    return dispatch_x<2, false>(h, gu, ntheta, j, st, data, partials, inv_norm, inv_beta_ratio);
+}
+
+extern "C" int mm_prop_grad_backward(mm_prop* h, const void* gu, const float* proj, float inv_norm,
+                                     float inv_beta_ratio, float* gp, int ntheta, int j, void* stream) {
+    MM_TRY(check_call(h, gu, gp, ntheta, j, "mm_prop_grad_backward"));
+    MM_REQUIRE(proj != nullptr, "mm_prop_grad_backward: NULL proj");
+    cudaStream_t st = (cudaStream_t)stream;
+    MM_TRY((dispatch_y<0, true>(h, gu, ntheta, j, 0.f, 0.f, st)));
+    return dispatch_x<3, true>(h, gp, ntheta, j, st, proj, nullptr, inv_norm, inv_beta_ratio);
 }

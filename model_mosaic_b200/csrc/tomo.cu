@@ -19,6 +19,7 @@
 //    static CSR table (destination cell -> (sample, weight, conj)) built once
 //    by a radix sort of (cell, sample, tap) keys: deterministic, no atomics.
 #include "mm_common.cuh"
+#include "fft_smem.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 #include <math.h>
@@ -35,6 +36,7 @@ struct mm_tomo {
     float* d_cos = nullptr;
     float* d_sin = nullptr;
     float* d_phi1 = nullptr;
+    float2* d_twy = nullptr;     // Stockham twiddles of the 2n-point column transform
     // forward buffers
     float* P = nullptr;          // (zs, n, 2n)     padded phi*obj rows
     float2* X = nullptr;         // (zs, n, n+1)    row spectra
@@ -204,10 +206,39 @@ __global__ void k_transpose_out(const float2* __restrict__ B, float2* __restrict
     }
 }
 
+// R stage 4 / RT y-IFFT: length-2n transforms along v of the slice-
+// interleaved spectrum, 4 adjacent (u, z) columns per block so every row
+// access is one 32-byte sector.  Forward: rows outside [n/2, 3n/2) are the
+// zero padding and are not read.  Inverse: only rows [n/2, 3n/2) are stored
+// (the x-C2R needs nothing else).  src/dst row stride = (n+1)*zs.
+template <int L, bool INV>
+__global__ void __launch_bounds__(4 * stockham::Sched<L>::G) k_col_fft(const float2* __restrict__ src,
+                                                                           float2* __restrict__ dst,
+                                                                           const float2* __restrict__ tw,
+                                                                           long ncols) {
+    namespace sk = stockham;
+    constexpr int CW = 4;
+    extern __shared__ float2 sm[];
+    const int c = threadIdx.x, g = threadIdx.y;
+    const long col = (long)blockIdx.x * CW + c;
+    const bool live = col < ncols;
+    const int n = L / 2;
+    const sk::ColAddr<CW> ad{c};
+    auto ld = [&](int pos) -> float2 {
+        if (!INV && (pos < n / 2 || pos >= 3 * n / 2)) return make_float2(0.f, 0.f);
+        return live ? __ldg(src + (long)pos * ncols + col) : make_float2(0.f, 0.f);
+    };
+    auto st = [&](int pos, float2 v) {
+        if (INV && (pos < n / 2 || pos >= 3 * n / 2)) return;
+        if (live) dst[(long)pos * ncols + col] = v;
+    };
+    sk::fft<L, INV>(sm, ad, ld, st, g, tw);
+}
+
 // R stage 5: Gaussian gather of the n/2+1 non-redundant samples per angle.
 // One group of LPS lanes per sample; each lane owns ZV slices.
 template <int ZV, int LPS, int M>
-__global__ void __launch_bounds__(kThreads) k_gather(const float2* __restrict__ F, float2* __restrict__ H,
+__global__ void __launch_bounds__(kThreads, 4) k_gather(const float2* __restrict__ F, float2* __restrict__ H,
                                                      const float* __restrict__ cosT, const float* __restrict__ sinT,
                                                      int n, int T, int zs, float c0, float c1, float scale,
                                                      int clamp) {
@@ -304,6 +335,55 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict
 #pragma unroll
     for (int q = 0; q < 2 * ZV; ++q) acc[q] = 0.f;
     const unsigned e0 = __ldg(ptr + c), e1 = __ldg(ptr + c + 1);
+    if constexpr (LPS == 32) {
+        // one cell per warp: 32 table entries per coalesced load, handed out
+        // by shuffles, four independent value loads in flight
+        const unsigned FULL = 0xffffffffu;
+        for (unsigned base = e0; base < e1; base += 32) {
+            const int cnt = (int)min(32u, e1 - base);
+            unsigned mi = 0;
+            float mw = 0.f;
+            if (lane < cnt) {
+                mi = __ldg(idx + base + lane);
+                mw = __ldg(wgt + base + lane);
+            }
+            int k = 0;
+            for (; k + 4 <= cnt; k += 4) {
+                unsigned ii[4];
+                float ww[4], vv[4][2 * ZV];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    ii[u] = __shfl_sync(FULL, mi, k + u);
+                    ww[u] = __shfl_sync(FULL, mw, k + u);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) ZVec<ZV>::load(Q + (long)(ii[u] & 0x7fffffffu) * zs + zoff, vv[u]);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const float sw = (ii[u] >> 31) ? -ww[u] : ww[u];
+#pragma unroll
+                    for (int q = 0; q < 2 * ZV; q += 2) {
+                        acc[q] = fmaf(ww[u], vv[u][q], acc[q]);
+                        acc[q + 1] = fmaf(sw, vv[u][q + 1], acc[q + 1]);
+                    }
+                }
+            }
+            for (; k < cnt; ++k) {
+                const unsigned ia = __shfl_sync(FULL, mi, k);
+                const float wa = __shfl_sync(FULL, mw, k);
+                float va[2 * ZV];
+                ZVec<ZV>::load(Q + (long)(ia & 0x7fffffffu) * zs + zoff, va);
+                const float sa = (ia >> 31) ? -wa : wa;
+#pragma unroll
+                for (int q = 0; q < 2 * ZV; q += 2) {
+                    acc[q] = fmaf(wa, va[q], acc[q]);
+                    acc[q + 1] = fmaf(sa, va[q + 1], acc[q + 1]);
+                }
+            }
+        }
+        ZVec<ZV>::store(A + c * zs + zoff, acc);
+        return;
+    }
     unsigned e = e0;
     for (; e + 2 <= e1; e += 2) {
         const unsigned ia = __ldg(idx + e), ib = __ldg(idx + e + 1);
@@ -502,6 +582,37 @@ int alloc(mm_tomo* h, Tp** p, size_t count, const char* what) {
     return MM_OK;
 }
 
+template <int L, bool INV>
+int launch_col_fft_l(mm_tomo* h, const float2* src, float2* dst, cudaStream_t st) {
+    namespace sk = stockham;
+    constexpr int CW = 4, G = sk::Sched<L>::G;
+    const long ncols = (long)(h->n + 1) * h->zs;
+    const size_t smem = (size_t)sk::ColAddr<CW>::rows(L) * CW * sizeof(float2);
+    auto kern = k_col_fft<L, INV>;
+    MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 block(CW, G), grid((unsigned)((ncols + CW - 1) / CW));
+    kern<<<grid, block, smem, st>>>(src, dst, h->d_twy, ncols);
+    MM_LAUNCHED();
+    return MM_OK;
+}
+
+// Column transform along v (length 2n) of the slice-interleaved spectrum.
+template <bool INV>
+int launch_col_fft(mm_tomo* h, const float2* src, float2* dst, cudaStream_t st) {
+    switch (2 * h->n) {
+        case 16: return launch_col_fft_l<16, INV>(h, src, dst, st);
+        case 32: return launch_col_fft_l<32, INV>(h, src, dst, st);
+        case 64: return launch_col_fft_l<64, INV>(h, src, dst, st);
+        case 128: return launch_col_fft_l<128, INV>(h, src, dst, st);
+        case 256: return launch_col_fft_l<256, INV>(h, src, dst, st);
+        case 512: return launch_col_fft_l<512, INV>(h, src, dst, st);
+        case 1024: return launch_col_fft_l<1024, INV>(h, src, dst, st);
+        case 2048: return launch_col_fft_l<2048, INV>(h, src, dst, st);
+        case 4096: return launch_col_fft_l<4096, INV>(h, src, dst, st);
+    }
+    return -100;  // not a power of two in range: caller uses cuFFT
+}
+
 int pick_lanes(int zs, int& ZV, int& LPS) {
     if (zs >= 64) { ZV = 2; LPS = 32; }
     else { ZV = 1; LPS = zs; }
@@ -647,7 +758,7 @@ void destroy(mm_tomo* h) {
     cufftHandle all[6] = {h->plan_xr2c, h->plan_xc2r, h->plan_y, h->plan_rc2r, h->plan_rr2c, h->plan_rc2c};
     for (cufftHandle p : all)
         if (p) cufftDestroy(p);
-    void* bufs[] = {h->d_cos, h->d_sin, h->d_phi1, h->P, h->X, h->Y, h->F, h->Hh, h->sino_tmp, h->fft_work,
+    void* bufs[] = {h->d_cos, h->d_sin, h->d_phi1, h->d_twy, h->P, h->X, h->Y, h->F, h->Hh, h->sino_tmp, h->fft_work,
                     h->csr_ptr, h->csr_idx, h->csr_w, h->ypad, h->yc};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -704,6 +815,20 @@ extern "C" int mm_tomo_create(int n, int nz, int ntheta, const float* theta_host
     if ((rc = alloc(h, &h->d_cos, ntheta, "cos table")) || (rc = alloc(h, &h->d_sin, ntheta, "sin table")) ||
         (rc = alloc(h, &h->d_phi1, n, "phi table")))
         return fail(rc);
+    if (mm_is_pow2(2L * n) && 2 * n <= 4096) {
+        // the table of an L-point line has < 1.1 L entries; size it 2L
+        std::vector<float2> tw(4 * (size_t)n, make_float2(0.f, 0.f));
+        stockham::host_twiddles(2 * n, false, tw.data());
+        if ((rc = alloc(h, &h->d_twy, tw.size(), "column FFT twiddles"))) return fail(rc);
+        if (cudaMemcpy(h->d_twy, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess) {
+            mm::set_error("mm_tomo_create: table upload failed");
+            return fail(MM_ECUDA);
+        }
+        if (mmfft::init_constants() != cudaSuccess) {
+            mm::set_error("mm_tomo_create: FFT constant upload failed");
+            return fail(MM_ECUDA);
+        }
+    }
     if (cudaMemcpy(h->d_cos, cs.data(), ntheta * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(h->d_sin, sn.data(), ntheta * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(h->d_phi1, ph.data(), n * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
@@ -771,9 +896,14 @@ extern "C" int mm_tomo_R(mm_tomo* h, const float* obj, float* sino, int nz, void
     MM_LAUNCHED();
     h->tm.end(st, 1);
     h->tm.begin(3, st);
-    MM_CUFFT(cufftSetStream(h->plan_y, st));
-    MM_CUFFT(cufftExecC2C(h->plan_y, (cufftComplex*)h->Y, (cufftComplex*)h->F, CUFFT_FORWARD));
-    h->tm.end(st, 0);
+    int rc = launch_col_fft<false>(h, h->Y, h->F, st);
+    if (rc == -100) {
+        MM_CUFFT(cufftSetStream(h->plan_y, st));
+        MM_CUFFT(cufftExecC2C(h->plan_y, (cufftComplex*)h->Y, (cufftComplex*)h->F, CUFFT_FORWARD));
+    } else if (rc != MM_OK) {
+        return rc;
+    }
+    h->tm.end(st, rc == -100 ? 0 : 1);
     h->tm.begin(4, st);
     MM_TRY(launch_gather(h, st));
     h->tm.end(st, 1);
@@ -807,10 +937,15 @@ int rt_tail(mm_tomo* h, cudaStream_t st) {
     MM_TRY(launch_scatter(h, h->Hh, h->F, st));
     h->tm.end(st, 1);
     h->tm.begin(8, st);
-    MM_CUFFT(cufftSetStream(h->plan_y, st));
-    MM_CUFFT(cufftExecC2C(h->plan_y, (cufftComplex*)h->F, (cufftComplex*)h->Y, CUFFT_INVERSE));
-    h->y_dirty = true;
-    h->tm.end(st, 0);
+    int rc = launch_col_fft<true>(h, h->F, h->Y, st);
+    if (rc == -100) {
+        MM_CUFFT(cufftSetStream(h->plan_y, st));
+        MM_CUFFT(cufftExecC2C(h->plan_y, (cufftComplex*)h->F, (cufftComplex*)h->Y, CUFFT_INVERSE));
+        h->y_dirty = true;
+    } else if (rc != MM_OK) {
+        return rc;
+    }
+    h->tm.end(st, rc == -100 ? 0 : 1);
     h->tm.begin(9, st);
     dim3 tb(32, 8), tg((n + 1 + 31) / 32, (zs + 31) / 32, n);
     k_transpose_out<<<tg, tb, 0, st>>>(h->Y, h->X, n, zs);

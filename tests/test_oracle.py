@@ -99,3 +99,20 @@ def test_psi_abs2():
     ph = p * 0.5
     assert np.allclose(psi, np.exp(-ph * 0.01) * np.exp(1j * ph))
     assert np.allclose(abs2(psi), np.exp(-2 * ph * 0.01))
+
+
+def test_model_oracle_gradient_vs_central_differences():
+    # FP64 check of the chain rule used by the hand-written backward
+    from oracle.model import ModelOracle
+    n, nz, T = 32, 4, 24
+    theta = np.linspace(0, np.pi, T, endpoint=False).astype(np.float32)
+    rng = np.random.default_rng(0)
+    m = ModelOracle(n, nz, theta, 4.133e-11, 0.69e-6, 0.12, s=40.0)
+    delta = rng.uniform(0, 1, (nz, n, n)) * 1e-2
+    d = m.forward(rng.uniform(0, 1, (nz, n, n)) * 1e-2)
+    g = m.grad(delta, d)
+    for _ in range(3):
+        v = rng.standard_normal(delta.shape)
+        h = 1e-6
+        fd = (m.loss(delta + h * v, d) - m.loss(delta - h * v, d)) / (2 * h)
+        assert abs(np.sum(g * v) - fd) / abs(fd) < 1e-7
