@@ -36,7 +36,10 @@ struct mm_tomo {
     float* d_cos = nullptr;
     float* d_sin = nullptr;
     float* d_phi1 = nullptr;
-    float2* d_twy = nullptr;     // Stockham twiddles of the 2n-point column transform
+    float2* d_twy = nullptr;     // Stockham twiddles of the 2n-point x and column transforms
+    float2* d_twr = nullptr;     // Stockham twiddles of the n/2-point r transforms
+    float2* d_exr = nullptr;     // e^{+2 pi i k/n}, k = 0..n/2 (real-from-half-length packing)
+    bool fused_x = false, fused_r = false;
     // forward buffers
     float* P = nullptr;          // (zs, n, 2n)     padded phi*obj rows
     float2* X = nullptr;         // (zs, n, n+1)    row spectra
@@ -233,6 +236,200 @@ __global__ void __launch_bounds__(4 * stockham::Sched<L>::G) k_col_fft(const flo
         if (live) dst[(long)pos * ncols + col] = v;
     };
     sk::fft<L, INV>(sm, ad, ld, st, g, tw);
+}
+
+// ---------------------------------------------------------------------------
+// Fused x-side and r-side transforms (Stockham lines in shared memory).
+
+// R x-side: rows (z, y) of phi*obj, zero padded to L = 2n, real FFT with two
+// rows packed per complex line, written slice-interleaved into the centre
+// rows of Y[v][u][z] (four slices = one 32-byte sector per u).
+// Block (G, 2): line l holds rows z0 + 2l (real part) and z0 + 2l + 1 (imag).
+template <int L>
+__global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xfwd(const float* __restrict__ obj,
+                                                                     float2* __restrict__ Y,
+                                                                     const float* __restrict__ phi1, float phis,
+                                                                     const float2* __restrict__ tw, int nzc,
+                                                                     int zs) {
+    constexpr int n = L / 2, LP = L + L / 16, G = stockham::Sched<L>::G;
+    extern __shared__ float2 sm[];
+    const int g = threadIdx.x, l = threadIdx.y;
+    const int y = blockIdx.x, z0 = blockIdx.y * 4;
+    const int za = z0 + 2 * l, zb = za + 1;
+    const stockham::RowAddr ad{l * LP};
+    const float py = phis * __ldg(phi1 + y);
+    const float* ra = obj + ((long)za * n + y) * n;
+    const float* rb = obj + ((long)zb * n + y) * n;
+    auto ld = [&](int pos) -> float2 {
+        const int x = pos - n / 2;
+        if (x < 0 || x >= n) return make_float2(0.f, 0.f);
+        const float w = py * __ldg(phi1 + x);
+        return make_float2(za < nzc ? w * __ldg(ra + x) : 0.f, zb < nzc ? w * __ldg(rb + x) : 0.f);
+    };
+    auto st = [&](int pos, float2 v) { sm[ad(pos)] = v; };
+    stockham::fft<L, false>(sm, ad, ld, st, g, tw);
+    __syncthreads();
+    const int tid = l * G + g;
+    const int nq = min(4, zs - z0);
+    // one thread per u: the four slices of one u are one 32-byte sector
+    for (int k = tid; k <= n; k += 2 * G) {
+        const int km = (L - k) & (L - 1);
+        float2 v[4];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const float2 zk = sm[h * LP + k + (k >> 4)];
+            const float2 zm = sm[h * LP + km + (km >> 4)];
+            // A = (Zk + conj Zm)/2 (real row), B = (Zk - conj Zm)/(2i) (imag row)
+            v[2 * h] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+            v[2 * h + 1] = make_float2(0.5f * (zk.y + zm.y), 0.5f * (zm.x - zk.x));
+        }
+        float2* dst = Y + ((long)(y + n / 2) * (n + 1) + k) * zs + z0;
+        if (nq == 4) {
+            reinterpret_cast<float4*>(dst)[0] = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+            reinterpret_cast<float4*>(dst)[1] = make_float4(v[2].x, v[2].y, v[3].x, v[3].y);
+        } else {
+            for (int q = 0; q < nq; ++q) dst[q] = v[q];
+        }
+    }
+}
+
+// RT x-side: centre rows of B[v][u][z] for one y and four slices -> halve
+// the interior columns (transpose of the x real FFT), real parts only at
+// u = 0 and u = n, two rows packed per complex inverse line, crop to
+// [n/2, 3n/2), times phi.  OUT 0: float obj; 1/2: real/imag part of complex.
+template <int L, int OUT>
+__global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xinv(const float2* __restrict__ B,
+                                                                     void* __restrict__ obj,
+                                                                     const float* __restrict__ phi1, float phis,
+                                                                     const float2* __restrict__ tw, int nzc,
+                                                                     int zs) {
+    constexpr int n = L / 2, LP = L + L / 16, G = stockham::Sched<L>::G;
+    extern __shared__ float2 sm[];
+    const int g = threadIdx.x, l = threadIdx.y;
+    const int y = blockIdx.x, z0 = blockIdx.y * 4;
+    const int tid = l * G + g;
+    const int nq = min(4, zs - z0);
+    // one thread per u: load the four slices (one 32-byte sector), line h
+    // gets Z = A + iB from rows 2h (A) and 2h + 1 (B)
+    for (int k = tid; k <= n; k += 2 * G) {
+        const float2* src = B + ((long)(y + n / 2) * (n + 1) + k) * zs + z0;
+        float2 v[4];
+        if (nq == 4) {
+            const float4 a = __ldg(reinterpret_cast<const float4*>(src));
+            const float4 b = __ldg(reinterpret_cast<const float4*>(src) + 1);
+            v[0] = make_float2(a.x, a.y); v[1] = make_float2(a.z, a.w);
+            v[2] = make_float2(b.x, b.y); v[3] = make_float2(b.z, b.w);
+        } else {
+            for (int q = 0; q < 4; ++q) v[q] = q < nq ? __ldg(src + q) : make_float2(0.f, 0.f);
+        }
+        const bool interior = k > 0 && k < n;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (interior) { v[q].x *= 0.5f; v[q].y *= 0.5f; } else { v[q].y = 0.f; }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const float2 A = v[2 * h], Bv = v[2 * h + 1];
+            sm[h * LP + k + (k >> 4)] = make_float2(A.x - Bv.y, A.y + Bv.x);              // A + iB
+            if (interior) {
+                const int km = L - k;
+                sm[h * LP + km + (km >> 4)] = make_float2(A.x + Bv.y, Bv.x - A.y);        // conj A + i conj B
+            }
+        }
+    }
+    __syncthreads();
+    const stockham::RowAddr ad{l * LP};
+    const int za = z0 + 2 * l, zb = za + 1;
+    const float py = phis * __ldg(phi1 + y);
+    auto ld = [&](int pos) -> float2 { return sm[ad(pos)]; };
+    auto st = [&](int pos, float2 v) {
+        const int x = pos - n / 2;
+        if (x < 0 || x >= n) return;
+        const float w = py * __ldg(phi1 + x);
+        float* o = static_cast<float*>(obj);
+        if (OUT == 0) {
+            if (za < nzc) o[((long)za * n + y) * n + x] = w * v.x;
+            if (zb < nzc) o[((long)zb * n + y) * n + x] = w * v.y;
+        } else {
+            if (za < nzc) o[(((long)za * n + y) * n + x) * 2 + (OUT - 1)] = w * v.x;
+            if (zb < nzc) o[(((long)zb * n + y) * n + x) * 2 + (OUT - 1)] = w * v.y;
+        }
+    };
+    stockham::fft<L, true>(sm, ad, ld, st, g, tw);
+}
+
+// R r-side: C2R of length 2M along k for columns c of H[k][c] (k = 0..M),
+// as a complex inverse line of M points: Z[k] = (X[k] + conj X[M-k]) +
+// i e^{+2 pi i k/2M} (X[k] - conj X[M-k]); x[2m] = Re z[m], x[2m+1] = Im z[m].
+// Block (G, 8): eight columns (64 bytes per k) per block.
+template <int M>
+__global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rc2r(const float2* __restrict__ H,
+                                                                     float* __restrict__ out,
+                                                                     const float2* __restrict__ tw,
+                                                                     const float2* __restrict__ ex, long C) {
+    constexpr int CB = 8, LP = M + M / 16, G = stockham::Sched<M>::G;
+    extern __shared__ float2 sm[];
+    const int g = threadIdx.x, l = threadIdx.y;
+    const long c0 = (long)blockIdx.x * CB;
+    const int tid = l * G + g;
+    float2* stg = sm;  // [CB][M + 1]; aliased by the line buffers after pass 0 reads
+    for (int idx = tid; idx < (M + 1) * CB; idx += CB * G) {
+        const int c = idx & (CB - 1), k = idx >> 3;
+        stg[c * (M + 1) + k] = (c0 + c < C) ? __ldg(H + (long)k * C + c0 + c) : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const stockham::RowAddr ad{l * LP};
+    const float2* X = stg + l * (M + 1);
+    auto ld = [&](int pos) -> float2 {
+        const float2 a = X[pos], b = X[M - pos];
+        const float2 e = make_float2(a.x + b.x, a.y - b.y);            // X[k] + conj X[M-k]
+        const float2 d = make_float2(a.x - b.x, a.y + b.y);            // X[k] - conj X[M-k]
+        const float2 w = __ldg(ex + pos);                               // e^{+2 pi i k / 2M}
+        const float2 od = make_float2(d.x * w.x - d.y * w.y, d.x * w.y + d.y * w.x);
+        return make_float2(e.x - od.y, e.y + od.x);                     // e + i od
+    };
+    float* orow = out + (c0 + l) * (2 * M);
+    const bool live = c0 + l < C;
+    auto st = [&](int pos, float2 v) {
+        if (live) *reinterpret_cast<float2*>(orow + 2 * pos) = v;
+    };
+    stockham::fft<M, true>(sm, ad, ld, st, g, tw);
+}
+
+// RT r-side: R2C of length 2M of real rows y[c][0..2M) as a complex forward
+// line z[m] = y[2m] + i y[2m+1]; X[k] = (Z[k] + conj Z[M-k])/2 +
+// e^{-2 pi i k/2M} (Z[k] - conj Z[M-k])/(2i) for k = 0..M, written to
+// H[k][c] (eight columns = 64 bytes per k).
+template <int M>
+__global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rr2c(const float* __restrict__ yv,
+                                                                     float2* __restrict__ H,
+                                                                     const float2* __restrict__ tw,
+                                                                     const float2* __restrict__ ex, long C) {
+    constexpr int CB = 8, LP = M + M / 16, G = stockham::Sched<M>::G;
+    extern __shared__ float2 sm[];
+    const int g = threadIdx.x, l = threadIdx.y;
+    const long c0 = (long)blockIdx.x * CB;
+    const bool live = c0 + l < C;
+    const float* row = yv + (c0 + l) * (2 * M);
+    const stockham::RowAddr ad{l * LP};
+    auto ld = [&](int pos) -> float2 {
+        return live ? __ldg(reinterpret_cast<const float2*>(row) + pos) : make_float2(0.f, 0.f);
+    };
+    auto st = [&](int pos, float2 v) { sm[ad(pos)] = v; };
+    stockham::fft<M, false>(sm, ad, ld, st, g, tw);
+    __syncthreads();
+    const int tid = l * G + g;
+    for (int idx = tid; idx < (M + 1) * CB; idx += CB * G) {
+        const int c = idx & (CB - 1), k = idx >> 3;
+        if (c0 + c >= C) continue;
+        const int kk = k & (M - 1), km = (M - k) & (M - 1);
+        const float2 a = sm[c * LP + kk + (kk >> 4)], b = sm[c * LP + km + (km >> 4)];
+        const float2 e = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));     // (Zk + conj Zm)/2
+        const float2 d = make_float2(0.5f * (a.y + b.y), 0.5f * (b.x - a.x));     // (Zk - conj Zm)/(2i)
+        const float2 w = __ldg(ex + k);                                           // e^{+2 pi i k / 2M}
+        const float2 od = make_float2(d.x * w.x + d.y * w.y, d.y * w.x - d.x * w.y);  // d * conj(w)
+        H[(long)k * C + c0 + c] = make_float2(e.x + od.x, e.y + od.y);
+    }
 }
 
 // R stage 5: Gaussian gather of the n/2+1 non-redundant samples per angle.
@@ -613,6 +810,90 @@ int launch_col_fft(mm_tomo* h, const float2* src, float2* dst, cudaStream_t st) 
     return -100;  // not a power of two in range: caller uses cuFFT
 }
 
+template <int L>
+int launch_xfwd_l(mm_tomo* h, const float* obj, int nzc, cudaStream_t st) {
+    constexpr int G = stockham::Sched<L>::G;
+    const size_t smem = (size_t)2 * (L + L / 16) * sizeof(float2);
+    auto kern = k_xfwd<L>;
+    MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 block(G, 2), grid(h->n, (h->zs + 3) / 4);
+    kern<<<grid, block, smem, st>>>(obj, h->Y, h->d_phi1, h->phi_scale, h->d_twy, nzc, h->zs);
+    MM_LAUNCHED();
+    return MM_OK;
+}
+
+template <int L, int OUT>
+int launch_xinv_l(mm_tomo* h, void* obj, int nzc, cudaStream_t st) {
+    constexpr int G = stockham::Sched<L>::G;
+    const size_t smem = (size_t)2 * (L + L / 16) * sizeof(float2);
+    auto kern = k_xinv<L, OUT>;
+    MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 block(G, 2), grid(h->n, (h->zs + 3) / 4);
+    kern<<<grid, block, smem, st>>>(h->Y, obj, h->d_phi1, h->phi_scale, h->d_twy, nzc, h->zs);
+    MM_LAUNCHED();
+    return MM_OK;
+}
+
+template <int M>
+int launch_r_l(mm_tomo* h, bool inv, const void* src, void* dst, cudaStream_t st) {
+    constexpr int G = stockham::Sched<M>::G;
+    const size_t smem = (size_t)8 * (M + M / 16 > M + 1 ? M + M / 16 : M + 1) * sizeof(float2);
+    const long C = (long)h->ntheta * h->zs;
+    dim3 block(G, 8), grid((unsigned)((C + 7) / 8));
+    if (inv) {
+        auto kern = k_rc2r<M>;
+        MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<grid, block, smem, st>>>((const float2*)src, (float*)dst, h->d_twr, h->d_exr, C);
+    } else {
+        auto kern = k_rr2c<M>;
+        MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<grid, block, smem, st>>>((const float*)src, (float2*)dst, h->d_twr, h->d_exr, C);
+    }
+    MM_LAUNCHED();
+    return MM_OK;
+}
+
+int launch_xfwd(mm_tomo* h, const float* obj, int nzc, cudaStream_t st) {
+    switch (2 * h->n) {
+        case 64: return launch_xfwd_l<64>(h, obj, nzc, st);
+        case 128: return launch_xfwd_l<128>(h, obj, nzc, st);
+        case 256: return launch_xfwd_l<256>(h, obj, nzc, st);
+        case 512: return launch_xfwd_l<512>(h, obj, nzc, st);
+        case 1024: return launch_xfwd_l<1024>(h, obj, nzc, st);
+        case 2048: return launch_xfwd_l<2048>(h, obj, nzc, st);
+        case 4096: return launch_xfwd_l<4096>(h, obj, nzc, st);
+    }
+    MM_REQUIRE(false, "x transform: unsupported n=%d", h->n);
+}
+
+template <int OUT>
+int launch_xinv(mm_tomo* h, void* obj, int nzc, cudaStream_t st) {
+    switch (2 * h->n) {
+        case 64: return launch_xinv_l<64, OUT>(h, obj, nzc, st);
+        case 128: return launch_xinv_l<128, OUT>(h, obj, nzc, st);
+        case 256: return launch_xinv_l<256, OUT>(h, obj, nzc, st);
+        case 512: return launch_xinv_l<512, OUT>(h, obj, nzc, st);
+        case 1024: return launch_xinv_l<1024, OUT>(h, obj, nzc, st);
+        case 2048: return launch_xinv_l<2048, OUT>(h, obj, nzc, st);
+        case 4096: return launch_xinv_l<4096, OUT>(h, obj, nzc, st);
+    }
+    MM_REQUIRE(false, "x transform: unsupported n=%d", h->n);
+}
+
+int launch_r(mm_tomo* h, bool inv, const void* src, void* dst, cudaStream_t st) {
+    switch (h->n / 2) {
+        case 16: return launch_r_l<16>(h, inv, src, dst, st);
+        case 32: return launch_r_l<32>(h, inv, src, dst, st);
+        case 64: return launch_r_l<64>(h, inv, src, dst, st);
+        case 128: return launch_r_l<128>(h, inv, src, dst, st);
+        case 256: return launch_r_l<256>(h, inv, src, dst, st);
+        case 512: return launch_r_l<512>(h, inv, src, dst, st);
+        case 1024: return launch_r_l<1024>(h, inv, src, dst, st);
+        case 2048: return launch_r_l<2048>(h, inv, src, dst, st);
+    }
+    MM_REQUIRE(false, "r transform: unsupported n=%d", h->n);
+}
+
 int pick_lanes(int zs, int& ZV, int& LPS) {
     if (zs >= 64) { ZV = 2; LPS = 32; }
     else { ZV = 1; LPS = zs; }
@@ -758,7 +1039,7 @@ void destroy(mm_tomo* h) {
     cufftHandle all[6] = {h->plan_xr2c, h->plan_xc2r, h->plan_y, h->plan_rc2r, h->plan_rr2c, h->plan_rc2c};
     for (cufftHandle p : all)
         if (p) cufftDestroy(p);
-    void* bufs[] = {h->d_cos, h->d_sin, h->d_phi1, h->d_twy, h->P, h->X, h->Y, h->F, h->Hh, h->sino_tmp, h->fft_work,
+    void* bufs[] = {h->d_cos, h->d_sin, h->d_phi1, h->d_twy, h->d_twr, h->d_exr, h->P, h->X, h->Y, h->F, h->Hh, h->sino_tmp, h->fft_work,
                     h->csr_ptr, h->csr_idx, h->csr_w, h->ypad, h->yc};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -824,6 +1105,25 @@ extern "C" int mm_tomo_create(int n, int nz, int ntheta, const float* theta_host
             mm::set_error("mm_tomo_create: table upload failed");
             return fail(MM_ECUDA);
         }
+        h->fused_x = 2 * n >= 64;
+        const int M = n / 2;
+        if (M >= 16) {
+            std::vector<float2> twr(2 * (size_t)M, make_float2(0.f, 0.f)), exr(M + 1);
+            stockham::host_twiddles(M, false, twr.data());
+            for (int k = 0; k <= M; ++k) {
+                const double a = 2.0 * M_PI * k / n;
+                exr[k] = make_float2((float)cos(a), (float)sin(a));
+            }
+            if ((rc = alloc(h, &h->d_twr, twr.size(), "r FFT twiddles")) ||
+                (rc = alloc(h, &h->d_exr, exr.size(), "r packing twiddles")))
+                return fail(rc);
+            if (cudaMemcpy(h->d_twr, twr.data(), twr.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(h->d_exr, exr.data(), exr.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess) {
+                mm::set_error("mm_tomo_create: table upload failed");
+                return fail(MM_ECUDA);
+            }
+            h->fused_r = true;
+        }
         if (mmfft::init_constants() != cudaSuccess) {
             mm::set_error("mm_tomo_create: FFT constant upload failed");
             return fail(MM_ECUDA);
@@ -883,18 +1183,23 @@ extern "C" int mm_tomo_R(mm_tomo* h, const float* obj, float* sino, int nz, void
         MM_CUDA(cudaMemsetAsync(h->Y + (size_t)(3 * n / 2) * (n + 1) * zs, 0, half, st));
         h->y_dirty = false;
     }
-    k_pad_phi<<<(unsigned)((long)zs * n), kThreads, 0, st>>>(obj, h->P, h->d_phi1, h->phi_scale, n, nz);
-    MM_LAUNCHED();
-    h->tm.end(st, 1);
-    h->tm.begin(1, st);
-    MM_CUFFT(cufftSetStream(h->plan_xr2c, st));
-    MM_CUFFT(cufftExecR2C(h->plan_xr2c, h->P, (cufftComplex*)h->X));
-    h->tm.end(st, 0);
-    h->tm.begin(2, st);
-    dim3 tb(32, 8), tg((n + 1 + 31) / 32, (zs + 31) / 32, n);
-    k_transpose_in<<<tg, tb, 0, st>>>(h->X, h->Y, n, zs);
-    MM_LAUNCHED();
-    h->tm.end(st, 1);
+    if (h->fused_x) {  // phi*pad + x real FFT + slice interleave in one pass
+        MM_TRY(launch_xfwd(h, obj, nz, st));
+        h->tm.end(st, 1);
+    } else {
+        k_pad_phi<<<(unsigned)((long)zs * n), kThreads, 0, st>>>(obj, h->P, h->d_phi1, h->phi_scale, n, nz);
+        MM_LAUNCHED();
+        h->tm.end(st, 1);
+        h->tm.begin(1, st);
+        MM_CUFFT(cufftSetStream(h->plan_xr2c, st));
+        MM_CUFFT(cufftExecR2C(h->plan_xr2c, h->P, (cufftComplex*)h->X));
+        h->tm.end(st, 0);
+        h->tm.begin(2, st);
+        dim3 tb(32, 8), tg((n + 1 + 31) / 32, (zs + 31) / 32, n);
+        k_transpose_in<<<tg, tb, 0, st>>>(h->X, h->Y, n, zs);
+        MM_LAUNCHED();
+        h->tm.end(st, 1);
+    }
     h->tm.begin(3, st);
     int rc = launch_col_fft<false>(h, h->Y, h->F, st);
     if (rc == -100) {
@@ -913,13 +1218,17 @@ extern "C" int mm_tomo_R(mm_tomo* h, const float* obj, float* sino, int nz, void
         if (!h->sino_tmp) MM_TRY(alloc(h, &h->sino_tmp, (size_t)T * zs * n, "padded sinogram"));
         dst = h->sino_tmp;
     }
-    MM_CUFFT(cufftSetStream(h->plan_rc2r, st));
-    MM_CUFFT(cufftExecC2R(h->plan_rc2r, (cufftComplex*)h->Hh, dst));
+    if (h->fused_r) {
+        MM_TRY(launch_r(h, true, h->Hh, dst, st));
+    } else {
+        MM_CUFFT(cufftSetStream(h->plan_rc2r, st));
+        MM_CUFFT(cufftExecC2R(h->plan_rc2r, (cufftComplex*)h->Hh, dst));
+    }
     if (nz < zs) {
         k_copy_z<<<(unsigned)((long)T * nz), kThreads, 0, st>>>(h->sino_tmp, sino, n, zs, nz, nz);
         MM_LAUNCHED();
     }
-    h->tm.end(st, nz < zs ? 1 : 0);
+    h->tm.end(st, (nz < zs ? 1 : 0) + (h->fused_r ? 1 : 0));
     return MM_OK;
 }
 
@@ -946,6 +1255,7 @@ int rt_tail(mm_tomo* h, cudaStream_t st) {
         return rc;
     }
     h->tm.end(st, rc == -100 ? 0 : 1);
+    if (h->fused_x) return MM_OK;  // the caller's x-side kernel reads Y directly
     h->tm.begin(9, st);
     dim3 tb(32, 8), tg((n + 1 + 31) / 32, (zs + 31) / 32, n);
     k_transpose_out<<<tg, tb, 0, st>>>(h->Y, h->X, n, zs);
@@ -979,13 +1289,21 @@ extern "C" int mm_tomo_RT(mm_tomo* h, const void* sino, int dtype, void* obj, in
             MM_LAUNCHED();
             y = h->ypad;
         }
-        MM_CUFFT(cufftSetStream(h->plan_rr2c, st));
-        MM_CUFFT(cufftExecR2C(h->plan_rr2c, (cufftReal*)y, (cufftComplex*)h->Hh));
-        h->tm.end(st, nz < zs ? 1 : 0);
+        if (h->fused_r) {
+            MM_TRY(launch_r(h, false, y, h->Hh, st));
+        } else {
+            MM_CUFFT(cufftSetStream(h->plan_rr2c, st));
+            MM_CUFFT(cufftExecR2C(h->plan_rr2c, (cufftReal*)y, (cufftComplex*)h->Hh));
+        }
+        h->tm.end(st, (nz < zs ? 1 : 0) + (h->fused_r ? 1 : 0));
         MM_TRY(rt_tail(h, st));
         h->tm.begin(11, st);
-        k_crop_phi<0><<<rows, kThreads, 0, st>>>(h->P, obj, h->d_phi1, h->phi_scale, n);
-        MM_LAUNCHED();
+        if (h->fused_x) {
+            MM_TRY(launch_xinv<0>(h, obj, nz, st));
+        } else {
+            k_crop_phi<0><<<rows, kThreads, 0, st>>>(h->P, obj, h->d_phi1, h->phi_scale, n);
+            MM_LAUNCHED();
+        }
         h->tm.end(st, 1);
         return MM_OK;
     }
@@ -1017,11 +1335,15 @@ extern "C" int mm_tomo_RT(mm_tomo* h, const void* sino, int dtype, void* obj, in
         h->tm.end(st, 1);
         MM_TRY(rt_tail(h, st));
         h->tm.begin(11, st);
-        if (part == 0)
-            k_crop_phi<1><<<rows, kThreads, 0, st>>>(h->P, obj, h->d_phi1, h->phi_scale, n);
-        else
-            k_crop_phi<2><<<rows, kThreads, 0, st>>>(h->P, obj, h->d_phi1, h->phi_scale, n);
-        MM_LAUNCHED();
+        if (h->fused_x) {
+            MM_TRY(part == 0 ? launch_xinv<1>(h, obj, nz, st) : launch_xinv<2>(h, obj, nz, st));
+        } else {
+            if (part == 0)
+                k_crop_phi<1><<<rows, kThreads, 0, st>>>(h->P, obj, h->d_phi1, h->phi_scale, n);
+            else
+                k_crop_phi<2><<<rows, kThreads, 0, st>>>(h->P, obj, h->d_phi1, h->phi_scale, n);
+            MM_LAUNCHED();
+        }
         h->tm.end(st, 1);
     }
     return MM_OK;
