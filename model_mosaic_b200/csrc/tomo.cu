@@ -373,9 +373,21 @@ __global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rc2r(const float2
     const long c0 = (long)blockIdx.x * CB;
     const int tid = l * G + g;
     float2* stg = sm;  // [CB][M + 1]; aliased by the line buffers after pass 0 reads
-    for (int idx = tid; idx < (M + 1) * CB; idx += CB * G) {
-        const int c = idx & (CB - 1), k = idx >> 3;
-        stg[c * (M + 1) + k] = (c0 + c < C) ? __ldg(H + (long)k * C + c0 + c) : make_float2(0.f, 0.f);
+    {
+        // all loads of this thread issued before any store (latency bound)
+        constexpr int PER = ((M + 1) * CB + CB * G - 1) / (CB * G);
+        float2 v[PER];
+#pragma unroll
+        for (int r = 0; r < PER; ++r) {
+            const int idx = tid + r * CB * G;
+            const int c = idx & (CB - 1), k = idx >> 3;
+            v[r] = (idx < (M + 1) * CB && c0 + c < C) ? __ldg(H + (long)k * C + c0 + c) : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int r = 0; r < PER; ++r) {
+            const int idx = tid + r * CB * G;
+            if (idx < (M + 1) * CB) stg[(idx & (CB - 1)) * (M + 1) + (idx >> 3)] = v[r];
+        }
     }
     __syncthreads();
     const stockham::RowAddr ad{l * LP};
