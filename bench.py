@@ -166,12 +166,7 @@ def run_ours(args, w, rank, world, local_rank):
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    from model_mosaic_b200.dist import max_over_ranks
 
     for _ in range(args.warmup):
         step()
