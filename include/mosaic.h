@@ -28,8 +28,9 @@ extern "C" {
 #define MM_ECUFFT    -4   /* cuFFT error */
 #define MM_ETIMEOUT  -5   /* a bounded device wait gave up */
 
-#define MM_F32 0
-#define MM_C64 1
+#define MM_F32  0
+#define MM_C64  1
+#define MM_BF16 2   /* bfloat16 storage; arithmetic stays float32 */
 
 typedef struct mm_tomo mm_tomo;
 typedef struct mm_prop mm_prop;
@@ -41,7 +42,8 @@ typedef struct mm_tomo_opts {
     int    m;          /* half-width override; <= 0 -> from eps (reference formula) */
     int    clamp_xy;   /* 1: clamp sample coordinates to [-1/2, 1/2 - 1e-5] in R as
                           TomoLargeReal's gather does (processing/kernels.py:478-481) */
-    int    reserved[5];
+    int    compensated;  /* 1: Kahan-compensated sums in the adjoint scatter */
+    int    reserved[4];
 } mm_tomo_opts;
 
 /* Library and error reporting. */
@@ -62,11 +64,17 @@ int mm_tomo_destroy(mm_tomo* h);
  *   (processing/tomo_large.py:344-368): obj (nz, n, n) f32 -> sino
  *   (ntheta, nz, n) f32, for 1 <= nz <= the handle's nz.  Device pointers. */
 int mm_tomo_R(mm_tomo* h, const float* obj, float* sino, int nz, void* stream);
+/* mm_tomo_R with a storage type per array (MM_F32 or MM_BF16 each): bfloat16
+ *   storage of the volume and/or the sinogram, float32 arithmetic.  No
+ *   reference counterpart (the reference stores float32 only). */
+int mm_tomo_R_ex(mm_tomo* h, const void* obj, int obj_dtype, void* sino, int sino_dtype, int nz,
+                 void* stream);
 
 /* Replaces TomoReal.RT (processing/tomo.py:153-188) and TomoLargeReal.RT
  *   (processing/tomo_large.py:582-630): sino (ntheta, nz, n) of `dtype`
- *   (MM_F32 or MM_C64) -> obj (nz, n, n) of the same dtype (real part only
- *   for MM_F32, as the reference).  Deterministic: no float atomics. */
+ *   (MM_F32, MM_C64 or MM_BF16) -> obj (nz, n, n) of the same dtype (real
+ *   part only for real input, as the reference).  Deterministic: no float
+ *   atomics. */
 int mm_tomo_RT(mm_tomo* h, const void* sino, int dtype, void* obj, int nz, void* stream);
 
 /* Builds the adjoint's static scatter table now instead of on the first RT

@@ -14,7 +14,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libmosaic.so")
 
 MM_OK, MM_EINVAL, MM_ENOMEM, MM_ECUDA, MM_ECUFFT, MM_ETIMEOUT = 0, -1, -2, -3, -4, -5
-MM_F32, MM_C64 = 0, 1
+MM_F32, MM_C64, MM_BF16 = 0, 1, 2
 
 _lib = None
 _lock = threading.Lock()
@@ -40,6 +40,7 @@ def _declare(L):
     L.mm_tomo_create.argtypes = [i, i, i, p, p, C.POINTER(p)]
     L.mm_tomo_destroy.argtypes = [p]
     L.mm_tomo_R.argtypes = [p, p, p, i, p]
+    L.mm_tomo_R_ex.argtypes = [p, p, i, p, i, i, p]
     L.mm_tomo_RT.argtypes = [p, p, i, p, i, p]
     L.mm_tomo_prepare_rt.argtypes = [p, p]
     L.mm_tomo_workspace_bytes.argtypes = [p]
@@ -61,7 +62,7 @@ def _declare(L):
     L.mm_prop_D_noalloc.argtypes = [i, i, i, d, d, d, p, p, p]
     for name in ("mm_prop_grad_forward", "mm_prop_grad_backward", "mm_prop_D_noalloc",
                  "mm_tomo_set_timing", "mm_tomo_get_timing", "mm_prop_set_timing", "mm_prop_get_timing",
-                 "mm_tomo_create", "mm_tomo_destroy", "mm_tomo_R", "mm_tomo_RT", "mm_tomo_prepare_rt",
+                 "mm_tomo_create", "mm_tomo_destroy", "mm_tomo_R", "mm_tomo_R_ex", "mm_tomo_RT", "mm_tomo_prepare_rt",
                  "mm_prop_create", "mm_prop_destroy", "mm_prop_D", "mm_prop_DT", "mm_prop_intensity"):
         getattr(L, name).restype = i
     return L

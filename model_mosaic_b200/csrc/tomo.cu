@@ -22,6 +22,7 @@
 #include "fft_smem.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cuda_bf16.h>
 #include <math.h>
 
 #include <algorithm>
@@ -30,7 +31,7 @@
 using mm::dev_alloc;
 
 struct mm_tomo {
-    int n = 0, nz = 0, ntheta = 0, m = 0, zs = 0, K = 0, clamp = 0;
+    int n = 0, nz = 0, ntheta = 0, m = 0, zs = 0, K = 0, clamp = 0, compensated = 0;
     float mu = 0.f, c0 = 0.f, c1 = 0.f, phi_scale = 0.f;
     int device = 0;
     float* d_cos = nullptr;
@@ -124,6 +125,21 @@ __device__ __forceinline__ void tap_cell(int u, int v, int n, int& row, int& col
         cj = true;
     }
     row = v < 0 ? v + twon : (v >= twon ? v - twon : v);
+}
+
+// float32 or bfloat16 storage of the volume and the sinogram; arithmetic is
+// float32 either way.
+__device__ __forceinline__ float ld_elem(const float* p) { return __ldg(p); }
+__device__ __forceinline__ float ld_elem(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+__device__ __forceinline__ void st_elem(float* p, float v) { *p = v; }
+__device__ __forceinline__ void st_elem(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+__device__ __forceinline__ float2 ld_pair(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+__device__ __forceinline__ float2 ld_pair(const __nv_bfloat16* p) {
+    return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+}
+__device__ __forceinline__ void st_pair(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
+__device__ __forceinline__ void st_pair(__nv_bfloat16* p, float2 v) {
+    *reinterpret_cast<__nv_bfloat162*>(p) = __float22bfloat162_rn(v);
 }
 
 template <int ZV>
@@ -245,8 +261,8 @@ __global__ void __launch_bounds__(4 * stockham::Sched<L>::G) k_col_fft(const flo
 // rows packed per complex line, written slice-interleaved into the centre
 // rows of Y[v][u][z] (four slices = one 32-byte sector per u).
 // Block (G, 2): line l holds rows z0 + 2l (real part) and z0 + 2l + 1 (imag).
-template <int L>
-__global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xfwd(const float* __restrict__ obj,
+template <int L, typename TIN>
+__global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xfwd(const TIN* __restrict__ obj,
                                                                      float2* __restrict__ Y,
                                                                      const float* __restrict__ phi1, float phis,
                                                                      const float2* __restrict__ tw, int nzc,
@@ -258,13 +274,13 @@ __global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xfwd(const float*
     const int za = z0 + 2 * l, zb = za + 1;
     const stockham::RowAddr ad{l * LP};
     const float py = phis * __ldg(phi1 + y);
-    const float* ra = obj + ((long)za * n + y) * n;
-    const float* rb = obj + ((long)zb * n + y) * n;
+    const TIN* ra = obj + ((long)za * n + y) * n;
+    const TIN* rb = obj + ((long)zb * n + y) * n;
     auto ld = [&](int pos) -> float2 {
         const int x = pos - n / 2;
         if (x < 0 || x >= n) return make_float2(0.f, 0.f);
         const float w = py * __ldg(phi1 + x);
-        return make_float2(za < nzc ? w * __ldg(ra + x) : 0.f, zb < nzc ? w * __ldg(rb + x) : 0.f);
+        return make_float2(za < nzc ? w * ld_elem(ra + x) : 0.f, zb < nzc ? w * ld_elem(rb + x) : 0.f);
     };
     auto st = [&](int pos, float2 v) { sm[ad(pos)] = v; };
     stockham::fft<L, false>(sm, ad, ld, st, g, tw);
@@ -297,7 +313,7 @@ __global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xfwd(const float*
 // the interior columns (transpose of the x real FFT), real parts only at
 // u = 0 and u = n, two rows packed per complex inverse line, crop to
 // [n/2, 3n/2), times phi.  OUT 0: float obj; 1/2: real/imag part of complex.
-template <int L, int OUT>
+template <int L, int OUT, typename TOUT = float>
 __global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xinv(const float2* __restrict__ B,
                                                                      void* __restrict__ obj,
                                                                      const float* __restrict__ phi1, float phis,
@@ -346,11 +362,12 @@ __global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xinv(const float2
         const int x = pos - n / 2;
         if (x < 0 || x >= n) return;
         const float w = py * __ldg(phi1 + x);
-        float* o = static_cast<float*>(obj);
         if (OUT == 0) {
-            if (za < nzc) o[((long)za * n + y) * n + x] = w * v.x;
-            if (zb < nzc) o[((long)zb * n + y) * n + x] = w * v.y;
+            TOUT* o = static_cast<TOUT*>(obj);
+            if (za < nzc) st_elem(o + ((long)za * n + y) * n + x, w * v.x);
+            if (zb < nzc) st_elem(o + ((long)zb * n + y) * n + x, w * v.y);
         } else {
+            float* o = static_cast<float*>(obj);
             if (za < nzc) o[(((long)za * n + y) * n + x) * 2 + (OUT - 1)] = w * v.x;
             if (zb < nzc) o[(((long)zb * n + y) * n + x) * 2 + (OUT - 1)] = w * v.y;
         }
@@ -362,9 +379,9 @@ __global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xinv(const float2
 // as a complex inverse line of M points: Z[k] = (X[k] + conj X[M-k]) +
 // i e^{+2 pi i k/2M} (X[k] - conj X[M-k]); x[2m] = Re z[m], x[2m+1] = Im z[m].
 // Block (G, 8): eight columns (64 bytes per k) per block.
-template <int M>
+template <int M, typename TOUT>
 __global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rc2r(const float2* __restrict__ H,
-                                                                     float* __restrict__ out,
+                                                                     TOUT* __restrict__ out,
                                                                      const float2* __restrict__ tw,
                                                                      const float2* __restrict__ ex, long C) {
     constexpr int CB = 8, LP = M + M / 16, G = stockham::Sched<M>::G;
@@ -400,10 +417,10 @@ __global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rc2r(const float2
         const float2 od = make_float2(d.x * w.x - d.y * w.y, d.x * w.y + d.y * w.x);
         return make_float2(e.x - od.y, e.y + od.x);                     // e + i od
     };
-    float* orow = out + (c0 + l) * (2 * M);
+    TOUT* orow = out + (c0 + l) * (2 * M);
     const bool live = c0 + l < C;
     auto st = [&](int pos, float2 v) {
-        if (live) *reinterpret_cast<float2*>(orow + 2 * pos) = v;
+        if (live) st_pair(orow + 2 * pos, v);
     };
     stockham::fft<M, true>(sm, ad, ld, st, g, tw);
 }
@@ -412,8 +429,8 @@ __global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rc2r(const float2
 // line z[m] = y[2m] + i y[2m+1]; X[k] = (Z[k] + conj Z[M-k])/2 +
 // e^{-2 pi i k/2M} (Z[k] - conj Z[M-k])/(2i) for k = 0..M, written to
 // H[k][c] (eight columns = 64 bytes per k).
-template <int M>
-__global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rr2c(const float* __restrict__ yv,
+template <int M, typename TIN>
+__global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rr2c(const TIN* __restrict__ yv,
                                                                      float2* __restrict__ H,
                                                                      const float2* __restrict__ tw,
                                                                      const float2* __restrict__ ex, long C) {
@@ -422,11 +439,9 @@ __global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rr2c(const float*
     const int g = threadIdx.x, l = threadIdx.y;
     const long c0 = (long)blockIdx.x * CB;
     const bool live = c0 + l < C;
-    const float* row = yv + (c0 + l) * (2 * M);
+    const TIN* row = yv + (c0 + l) * (2 * M);
     const stockham::RowAddr ad{l * LP};
-    auto ld = [&](int pos) -> float2 {
-        return live ? __ldg(reinterpret_cast<const float2*>(row) + pos) : make_float2(0.f, 0.f);
-    };
+    auto ld = [&](int pos) -> float2 { return live ? ld_pair(row + 2 * pos) : make_float2(0.f, 0.f); };
     auto st = [&](int pos, float2 v) { sm[ad(pos)] = v; };
     stockham::fft<M, false>(sm, ad, ld, st, g, tw);
     __syncthreads();
@@ -524,8 +539,22 @@ __global__ void __launch_bounds__(kThreads, 4) k_gather(const float2* __restrict
     ZVec<ZV>::store(H + ((long)k * T + t) * zs + zoff, acc);
 }
 
+// One term w*v of a scatter sum; KAHAN keeps a running compensation c of the
+// rounding error of each addition (Kahan 1965), the rest is a plain FMA.
+template <bool KAHAN>
+__device__ __forceinline__ void acc_add(float& s, float& c, float w, float v) {
+    if constexpr (KAHAN) {
+        const float y = fmaf(w, v, -c);
+        const float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    } else {
+        s = fmaf(w, v, s);
+    }
+}
+
 // RT: pull-scatter over the static CSR table.  One lane group per cell.
-template <int ZV, int LPS>
+template <int ZV, int LPS, bool KAHAN>
 __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict__ ptr,
                                                       const unsigned* __restrict__ idx,
                                                       const float* __restrict__ wgt,
@@ -540,9 +569,9 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict
     const long c = (warp / zgroups) * SPW + sub;
     if (c >= ncells) return;
     const int zoff = (int)zg * (LPS * ZV) + zl * ZV;
-    float acc[2 * ZV];
+    float acc[2 * ZV], cmp[2 * ZV];
 #pragma unroll
-    for (int q = 0; q < 2 * ZV; ++q) acc[q] = 0.f;
+    for (int q = 0; q < 2 * ZV; ++q) acc[q] = cmp[q] = 0.f;
     const unsigned e0 = __ldg(ptr + c), e1 = __ldg(ptr + c + 1);
     if constexpr (LPS == 32) {
         // one cell per warp: 32 table entries per coalesced load, handed out
@@ -572,8 +601,8 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict
                     const float sw = (ii[u] >> 31) ? -ww[u] : ww[u];
 #pragma unroll
                     for (int q = 0; q < 2 * ZV; q += 2) {
-                        acc[q] = fmaf(ww[u], vv[u][q], acc[q]);
-                        acc[q + 1] = fmaf(sw, vv[u][q + 1], acc[q + 1]);
+                        acc_add<KAHAN>(acc[q], cmp[q], ww[u], vv[u][q]);
+                        acc_add<KAHAN>(acc[q + 1], cmp[q + 1], sw, vv[u][q + 1]);
                     }
                 }
             }
@@ -585,8 +614,8 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict
                 const float sa = (ia >> 31) ? -wa : wa;
 #pragma unroll
                 for (int q = 0; q < 2 * ZV; q += 2) {
-                    acc[q] = fmaf(wa, va[q], acc[q]);
-                    acc[q + 1] = fmaf(sa, va[q + 1], acc[q + 1]);
+                    acc_add<KAHAN>(acc[q], cmp[q], wa, va[q]);
+                    acc_add<KAHAN>(acc[q + 1], cmp[q + 1], sa, va[q + 1]);
                 }
             }
         }
@@ -603,13 +632,13 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict
         const float sa = (ia >> 31) ? -wa : wa, sb = (ib >> 31) ? -wb : wb;
 #pragma unroll
         for (int q = 0; q < 2 * ZV; q += 2) {
-            acc[q] = fmaf(wa, va[q], acc[q]);
-            acc[q + 1] = fmaf(sa, va[q + 1], acc[q + 1]);
+            acc_add<KAHAN>(acc[q], cmp[q], wa, va[q]);
+            acc_add<KAHAN>(acc[q + 1], cmp[q + 1], sa, va[q + 1]);
         }
 #pragma unroll
         for (int q = 0; q < 2 * ZV; q += 2) {
-            acc[q] = fmaf(wb, vb[q], acc[q]);
-            acc[q + 1] = fmaf(sb, vb[q + 1], acc[q + 1]);
+            acc_add<KAHAN>(acc[q], cmp[q], wb, vb[q]);
+            acc_add<KAHAN>(acc[q + 1], cmp[q + 1], sb, vb[q + 1]);
         }
     }
     if (e < e1) {
@@ -620,8 +649,8 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict
         const float sa = (ia >> 31) ? -wa : wa;
 #pragma unroll
         for (int q = 0; q < 2 * ZV; q += 2) {
-            acc[q] = fmaf(wa, va[q], acc[q]);
-            acc[q + 1] = fmaf(sa, va[q + 1], acc[q + 1]);
+            acc_add<KAHAN>(acc[q], cmp[q], wa, va[q]);
+            acc_add<KAHAN>(acc[q + 1], cmp[q + 1], sa, va[q + 1]);
         }
     }
     ZVec<ZV>::store(A + c * zs + zoff, acc);
@@ -712,6 +741,17 @@ __global__ void k_copy_z(const float* __restrict__ src, float* __restrict__ dst,
     const float* s = src + (t * zsrc + z) * n;
     for (int x = threadIdx.x; x < n; x += blockDim.x) d[x] = (z < zvalid) ? __ldg(s + x) : 0.f;
 }
+template <typename TI, typename TO>
+__global__ void k_copy_z_t(const TI* __restrict__ src, TO* __restrict__ dst, int n, int zsrc, int zdst,
+                           int zvalid) {
+    const long row = blockIdx.x;  // t * zdst + z
+    const int z = (int)(row % zdst);
+    const long t = row / zdst;
+    TO* d = dst + row * n;
+    const TI* s = src + (t * zsrc + z) * n;
+    for (int x = threadIdx.x; x < n; x += blockDim.x) st_elem(d + x, (z < zvalid) ? ld_elem(s + x) : 0.f);
+}
+
 __global__ void k_copy_z_c(const float2* __restrict__ src, float2* __restrict__ dst, int n, int zsrc, int zdst,
                            int zvalid) {
     const long row = blockIdx.x;
@@ -822,23 +862,23 @@ int launch_col_fft(mm_tomo* h, const float2* src, float2* dst, cudaStream_t st) 
     return -100;  // not a power of two in range: caller uses cuFFT
 }
 
-template <int L>
-int launch_xfwd_l(mm_tomo* h, const float* obj, int nzc, cudaStream_t st) {
+template <int L, typename TIN>
+int launch_xfwd_l(mm_tomo* h, const void* obj, int nzc, cudaStream_t st) {
     constexpr int G = stockham::Sched<L>::G;
     const size_t smem = (size_t)2 * (L + L / 16) * sizeof(float2);
-    auto kern = k_xfwd<L>;
+    auto kern = k_xfwd<L, TIN>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 block(G, 2), grid(h->n, (h->zs + 3) / 4);
-    kern<<<grid, block, smem, st>>>(obj, h->Y, h->d_phi1, h->phi_scale, h->d_twy, nzc, h->zs);
+    kern<<<grid, block, smem, st>>>((const TIN*)obj, h->Y, h->d_phi1, h->phi_scale, h->d_twy, nzc, h->zs);
     MM_LAUNCHED();
     return MM_OK;
 }
 
-template <int L, int OUT>
+template <int L, int OUT, typename TOUT>
 int launch_xinv_l(mm_tomo* h, void* obj, int nzc, cudaStream_t st) {
     constexpr int G = stockham::Sched<L>::G;
     const size_t smem = (size_t)2 * (L + L / 16) * sizeof(float2);
-    auto kern = k_xinv<L, OUT>;
+    auto kern = k_xinv<L, OUT, TOUT>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 block(G, 2), grid(h->n, (h->zs + 3) / 4);
     kern<<<grid, block, smem, st>>>(h->Y, obj, h->d_phi1, h->phi_scale, h->d_twy, nzc, h->zs);
@@ -846,64 +886,81 @@ int launch_xinv_l(mm_tomo* h, void* obj, int nzc, cudaStream_t st) {
     return MM_OK;
 }
 
-template <int M>
+template <int M, typename TS>
 int launch_r_l(mm_tomo* h, bool inv, const void* src, void* dst, cudaStream_t st) {
     constexpr int G = stockham::Sched<M>::G;
     const size_t smem = (size_t)8 * (M + M / 16 > M + 1 ? M + M / 16 : M + 1) * sizeof(float2);
     const long C = (long)h->ntheta * h->zs;
     dim3 block(G, 8), grid((unsigned)((C + 7) / 8));
     if (inv) {
-        auto kern = k_rc2r<M>;
+        auto kern = k_rc2r<M, TS>;
         MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<grid, block, smem, st>>>((const float2*)src, (float*)dst, h->d_twr, h->d_exr, C);
+        kern<<<grid, block, smem, st>>>((const float2*)src, (TS*)dst, h->d_twr, h->d_exr, C);
     } else {
-        auto kern = k_rr2c<M>;
+        auto kern = k_rr2c<M, TS>;
         MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<grid, block, smem, st>>>((const float*)src, (float2*)dst, h->d_twr, h->d_exr, C);
+        kern<<<grid, block, smem, st>>>((const TS*)src, (float2*)dst, h->d_twr, h->d_exr, C);
     }
     MM_LAUNCHED();
     return MM_OK;
 }
 
-int launch_xfwd(mm_tomo* h, const float* obj, int nzc, cudaStream_t st) {
+template <typename TIN>
+int launch_xfwd_t(mm_tomo* h, const void* obj, int nzc, cudaStream_t st) {
     switch (2 * h->n) {
-        case 64: return launch_xfwd_l<64>(h, obj, nzc, st);
-        case 128: return launch_xfwd_l<128>(h, obj, nzc, st);
-        case 256: return launch_xfwd_l<256>(h, obj, nzc, st);
-        case 512: return launch_xfwd_l<512>(h, obj, nzc, st);
-        case 1024: return launch_xfwd_l<1024>(h, obj, nzc, st);
-        case 2048: return launch_xfwd_l<2048>(h, obj, nzc, st);
-        case 4096: return launch_xfwd_l<4096>(h, obj, nzc, st);
+        case 64: return launch_xfwd_l<64, TIN>(h, obj, nzc, st);
+        case 128: return launch_xfwd_l<128, TIN>(h, obj, nzc, st);
+        case 256: return launch_xfwd_l<256, TIN>(h, obj, nzc, st);
+        case 512: return launch_xfwd_l<512, TIN>(h, obj, nzc, st);
+        case 1024: return launch_xfwd_l<1024, TIN>(h, obj, nzc, st);
+        case 2048: return launch_xfwd_l<2048, TIN>(h, obj, nzc, st);
+        case 4096: return launch_xfwd_l<4096, TIN>(h, obj, nzc, st);
+    }
+    MM_REQUIRE(false, "x transform: unsupported n=%d", h->n);
+}
+
+int launch_xfwd(mm_tomo* h, const void* obj, int dtype, int nzc, cudaStream_t st) {
+    return dtype == MM_BF16 ? launch_xfwd_t<__nv_bfloat16>(h, obj, nzc, st) : launch_xfwd_t<float>(h, obj, nzc, st);
+}
+
+template <int OUT, typename TOUT>
+int launch_xinv_t(mm_tomo* h, void* obj, int nzc, cudaStream_t st) {
+    switch (2 * h->n) {
+        case 64: return launch_xinv_l<64, OUT, TOUT>(h, obj, nzc, st);
+        case 128: return launch_xinv_l<128, OUT, TOUT>(h, obj, nzc, st);
+        case 256: return launch_xinv_l<256, OUT, TOUT>(h, obj, nzc, st);
+        case 512: return launch_xinv_l<512, OUT, TOUT>(h, obj, nzc, st);
+        case 1024: return launch_xinv_l<1024, OUT, TOUT>(h, obj, nzc, st);
+        case 2048: return launch_xinv_l<2048, OUT, TOUT>(h, obj, nzc, st);
+        case 4096: return launch_xinv_l<4096, OUT, TOUT>(h, obj, nzc, st);
     }
     MM_REQUIRE(false, "x transform: unsupported n=%d", h->n);
 }
 
 template <int OUT>
-int launch_xinv(mm_tomo* h, void* obj, int nzc, cudaStream_t st) {
-    switch (2 * h->n) {
-        case 64: return launch_xinv_l<64, OUT>(h, obj, nzc, st);
-        case 128: return launch_xinv_l<128, OUT>(h, obj, nzc, st);
-        case 256: return launch_xinv_l<256, OUT>(h, obj, nzc, st);
-        case 512: return launch_xinv_l<512, OUT>(h, obj, nzc, st);
-        case 1024: return launch_xinv_l<1024, OUT>(h, obj, nzc, st);
-        case 2048: return launch_xinv_l<2048, OUT>(h, obj, nzc, st);
-        case 4096: return launch_xinv_l<4096, OUT>(h, obj, nzc, st);
-    }
-    MM_REQUIRE(false, "x transform: unsupported n=%d", h->n);
+int launch_xinv(mm_tomo* h, void* obj, int nzc, cudaStream_t st, int dtype = MM_F32) {
+    if (OUT == 0 && dtype == MM_BF16) return launch_xinv_t<0, __nv_bfloat16>(h, obj, nzc, st);
+    return launch_xinv_t<OUT, float>(h, obj, nzc, st);
 }
 
-int launch_r(mm_tomo* h, bool inv, const void* src, void* dst, cudaStream_t st) {
+template <typename TS>
+int launch_r_t(mm_tomo* h, bool inv, const void* src, void* dst, cudaStream_t st) {
     switch (h->n / 2) {
-        case 16: return launch_r_l<16>(h, inv, src, dst, st);
-        case 32: return launch_r_l<32>(h, inv, src, dst, st);
-        case 64: return launch_r_l<64>(h, inv, src, dst, st);
-        case 128: return launch_r_l<128>(h, inv, src, dst, st);
-        case 256: return launch_r_l<256>(h, inv, src, dst, st);
-        case 512: return launch_r_l<512>(h, inv, src, dst, st);
-        case 1024: return launch_r_l<1024>(h, inv, src, dst, st);
-        case 2048: return launch_r_l<2048>(h, inv, src, dst, st);
+        case 16: return launch_r_l<16, TS>(h, inv, src, dst, st);
+        case 32: return launch_r_l<32, TS>(h, inv, src, dst, st);
+        case 64: return launch_r_l<64, TS>(h, inv, src, dst, st);
+        case 128: return launch_r_l<128, TS>(h, inv, src, dst, st);
+        case 256: return launch_r_l<256, TS>(h, inv, src, dst, st);
+        case 512: return launch_r_l<512, TS>(h, inv, src, dst, st);
+        case 1024: return launch_r_l<1024, TS>(h, inv, src, dst, st);
+        case 2048: return launch_r_l<2048, TS>(h, inv, src, dst, st);
     }
     MM_REQUIRE(false, "r transform: unsupported n=%d", h->n);
+}
+
+// r-side transform; `dtype` is the storage type of the real sinogram side.
+int launch_r(mm_tomo* h, bool inv, const void* src, void* dst, cudaStream_t st, int dtype = MM_F32) {
+    return dtype == MM_BF16 ? launch_r_t<__nv_bfloat16>(h, inv, src, dst, st) : launch_r_t<float>(h, inv, src, dst, st);
 }
 
 int pick_lanes(int zs, int& ZV, int& LPS) {
@@ -953,7 +1010,8 @@ int launch_scatter_t(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) {
     const long ncells = 2L * h->n * (h->n + 1);
     const long warps = ((ncells + (32 / LPS) - 1) / (32 / LPS)) * (h->zs / (LPS * ZV));
     const long blocks = (warps * 32 + kThreads - 1) / kThreads;
-    k_scatter<ZV, LPS><<<blocks, kThreads, 0, st>>>(h->csr_ptr, h->csr_idx, h->csr_w, Q, A, ncells, h->zs);
+    auto kern = h->compensated ? k_scatter<ZV, LPS, true> : k_scatter<ZV, LPS, false>;
+    kern<<<blocks, kThreads, 0, st>>>(h->csr_ptr, h->csr_idx, h->csr_w, Q, A, ncells, h->zs);
     MM_LAUNCHED();
     return MM_OK;
 }
@@ -1081,6 +1139,7 @@ extern "C" int mm_tomo_create(int n, int nz, int ntheta, const float* theta_host
     h->m = m;
     h->K = n / 2 + 1;
     h->clamp = (opts && opts->clamp_xy) ? 1 : 0;
+    h->compensated = (opts && opts->compensated) ? 1 : 0;
     int zs = 1;
     while (zs < nz) zs <<= 1;
     h->zs = zs;
@@ -1181,10 +1240,15 @@ extern "C" int mm_tomo_destroy(mm_tomo* h) {
 
 extern "C" size_t mm_tomo_workspace_bytes(const mm_tomo* h) { return h ? h->ws_bytes : 0; }
 
-extern "C" int mm_tomo_R(mm_tomo* h, const float* obj, float* sino, int nz, void* stream) {
+extern "C" int mm_tomo_R_ex(mm_tomo* h, const void* obj, int obj_dtype, void* sino, int sino_dtype, int nz,
+                            void* stream) {
     MM_REQUIRE(h != nullptr, "mm_tomo_R: NULL handle");
     MM_REQUIRE(obj != nullptr && sino != nullptr, "mm_tomo_R: NULL array");
     MM_REQUIRE(nz >= 1 && nz <= h->nz, "mm_tomo_R: nz=%d outside [1, %d]", nz, h->nz);
+    MM_REQUIRE((obj_dtype == MM_F32 || obj_dtype == MM_BF16) && (sino_dtype == MM_F32 || sino_dtype == MM_BF16),
+               "mm_tomo_R: storage dtypes must be MM_F32 or MM_BF16");
+    MM_REQUIRE((obj_dtype == MM_F32 && sino_dtype == MM_F32) || (h->fused_x && h->fused_r),
+               "mm_tomo_R: bfloat16 storage needs n a power of two in [32, 2048]");
     MM_REQUIRE(((uintptr_t)obj % 4) == 0 && ((uintptr_t)sino % 4) == 0, "mm_tomo_R: misaligned array");
     cudaStream_t st = (cudaStream_t)stream;
     const int n = h->n, zs = h->zs, T = h->ntheta;
@@ -1196,10 +1260,11 @@ extern "C" int mm_tomo_R(mm_tomo* h, const float* obj, float* sino, int nz, void
         h->y_dirty = false;
     }
     if (h->fused_x) {  // phi*pad + x real FFT + slice interleave in one pass
-        MM_TRY(launch_xfwd(h, obj, nz, st));
+        MM_TRY(launch_xfwd(h, obj, obj_dtype, nz, st));
         h->tm.end(st, 1);
     } else {
-        k_pad_phi<<<(unsigned)((long)zs * n), kThreads, 0, st>>>(obj, h->P, h->d_phi1, h->phi_scale, n, nz);
+        k_pad_phi<<<(unsigned)((long)zs * n), kThreads, 0, st>>>((const float*)obj, h->P, h->d_phi1, h->phi_scale,
+                                                                 n, nz);
         MM_LAUNCHED();
         h->tm.end(st, 1);
         h->tm.begin(1, st);
@@ -1225,23 +1290,32 @@ extern "C" int mm_tomo_R(mm_tomo* h, const float* obj, float* sino, int nz, void
     MM_TRY(launch_gather(h, st));
     h->tm.end(st, 1);
     h->tm.begin(5, st);
-    float* dst = sino;
+    void* dst = sino;
     if (nz < zs) {
         if (!h->sino_tmp) MM_TRY(alloc(h, &h->sino_tmp, (size_t)T * zs * n, "padded sinogram"));
         dst = h->sino_tmp;
     }
+    const int dst_dtype = nz < zs ? MM_F32 : sino_dtype;
     if (h->fused_r) {
-        MM_TRY(launch_r(h, true, h->Hh, dst, st));
+        MM_TRY(launch_r(h, true, h->Hh, dst, st, dst_dtype));
     } else {
         MM_CUFFT(cufftSetStream(h->plan_rc2r, st));
-        MM_CUFFT(cufftExecC2R(h->plan_rc2r, (cufftComplex*)h->Hh, dst));
+        MM_CUFFT(cufftExecC2R(h->plan_rc2r, (cufftComplex*)h->Hh, (float*)dst));
     }
     if (nz < zs) {
-        k_copy_z<<<(unsigned)((long)T * nz), kThreads, 0, st>>>(h->sino_tmp, sino, n, zs, nz, nz);
+        if (sino_dtype == MM_BF16)
+            k_copy_z_t<float, __nv_bfloat16><<<(unsigned)((long)T * nz), kThreads, 0, st>>>(
+                h->sino_tmp, (__nv_bfloat16*)sino, n, zs, nz, nz);
+        else
+            k_copy_z<<<(unsigned)((long)T * nz), kThreads, 0, st>>>(h->sino_tmp, (float*)sino, n, zs, nz, nz);
         MM_LAUNCHED();
     }
     h->tm.end(st, (nz < zs ? 1 : 0) + (h->fused_r ? 1 : 0));
     return MM_OK;
+}
+
+extern "C" int mm_tomo_R(mm_tomo* h, const float* obj, float* sino, int nz, void* stream) {
+    return mm_tomo_R_ex(h, obj, MM_F32, sino, MM_F32, nz, stream);
 }
 
 extern "C" int mm_tomo_prepare_rt(mm_tomo* h, void* stream) {
@@ -1284,7 +1358,9 @@ int rt_tail(mm_tomo* h, cudaStream_t st) {
 extern "C" int mm_tomo_RT(mm_tomo* h, const void* sino, int dtype, void* obj, int nz, void* stream) {
     MM_REQUIRE(h != nullptr, "mm_tomo_RT: NULL handle");
     MM_REQUIRE(sino != nullptr && obj != nullptr, "mm_tomo_RT: NULL array");
-    MM_REQUIRE(dtype == MM_F32 || dtype == MM_C64, "mm_tomo_RT: dtype %d unsupported", dtype);
+    MM_REQUIRE(dtype == MM_F32 || dtype == MM_C64 || dtype == MM_BF16, "mm_tomo_RT: dtype %d unsupported", dtype);
+    MM_REQUIRE(dtype != MM_BF16 || (h->fused_x && h->fused_r),
+               "mm_tomo_RT: bfloat16 storage needs n a power of two in [32, 2048]");
     MM_REQUIRE(nz >= 1 && nz <= h->nz, "mm_tomo_RT: nz=%d outside [1, %d]", nz, h->nz);
     MM_REQUIRE(((uintptr_t)sino % (dtype == MM_C64 ? 8 : 4)) == 0 && ((uintptr_t)obj % 4) == 0,
                "mm_tomo_RT: misaligned array");
@@ -1292,17 +1368,23 @@ extern "C" int mm_tomo_RT(mm_tomo* h, const void* sino, int dtype, void* obj, in
     MM_TRY(ensure_rt(h, st));
     const int n = h->n, zs = h->zs, T = h->ntheta;
     const unsigned rows = (unsigned)((long)nz * n);
-    if (dtype == MM_F32) {
+    if (dtype == MM_F32 || dtype == MM_BF16) {
         h->tm.begin(6, st);
-        const float* y = static_cast<const float*>(sino);
+        const void* y = sino;
+        int ydt = dtype;
         if (nz < zs) {
             if (!h->ypad) MM_TRY(alloc(h, &h->ypad, (size_t)T * zs * n, "padded sinogram"));
-            k_copy_z<<<(unsigned)((long)T * zs), kThreads, 0, st>>>(y, h->ypad, n, nz, zs, nz);
+            if (dtype == MM_BF16)
+                k_copy_z_t<__nv_bfloat16, float><<<(unsigned)((long)T * zs), kThreads, 0, st>>>(
+                    (const __nv_bfloat16*)sino, h->ypad, n, nz, zs, nz);
+            else
+                k_copy_z<<<(unsigned)((long)T * zs), kThreads, 0, st>>>((const float*)sino, h->ypad, n, nz, zs, nz);
             MM_LAUNCHED();
             y = h->ypad;
+            ydt = MM_F32;
         }
         if (h->fused_r) {
-            MM_TRY(launch_r(h, false, y, h->Hh, st));
+            MM_TRY(launch_r(h, false, y, h->Hh, st, ydt));
         } else {
             MM_CUFFT(cufftSetStream(h->plan_rr2c, st));
             MM_CUFFT(cufftExecR2C(h->plan_rr2c, (cufftReal*)y, (cufftComplex*)h->Hh));
@@ -1311,7 +1393,7 @@ extern "C" int mm_tomo_RT(mm_tomo* h, const void* sino, int dtype, void* obj, in
         MM_TRY(rt_tail(h, st));
         h->tm.begin(11, st);
         if (h->fused_x) {
-            MM_TRY(launch_xinv<0>(h, obj, nz, st));
+            MM_TRY(launch_xinv<0>(h, obj, nz, st, dtype));
         } else {
             k_crop_phi<0><<<rows, kThreads, 0, st>>>(h->P, obj, h->d_phi1, h->phi_scale, n);
             MM_LAUNCHED();

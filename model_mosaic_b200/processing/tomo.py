@@ -15,7 +15,11 @@ All arithmetic runs in the CUDA library (``libmosaic.so``) through the C-ABI.
 Keyword-only extras (not in the reference): ``eps`` and ``m`` override the
 Gaussian accuracy / half-width (defaults 1e-3 and 4, processing/tomo.py:39-42);
 ``clamp_xy`` selects TomoLargeReal's clamped sample coordinates
-(processing/kernels.py:478-481).
+(processing/kernels.py:478-481); ``compensated`` makes the adjoint's sums
+Kahan-compensated.  bfloat16 torch tensors are accepted as storage (the
+arithmetic stays float32): ``R`` of a bfloat16 volume returns a bfloat16
+sinogram unless ``out_dtype`` says otherwise, ``RT`` of a bfloat16 sinogram
+returns a bfloat16 volume.
 """
 from __future__ import annotations
 
@@ -29,13 +33,19 @@ from model_mosaic_b200._interop import (require_cuda, to_device, from_device, st
 
 
 class _TomoOpts(C.Structure):
-    _fields_ = [("eps", C.c_double), ("m", C.c_int), ("clamp_xy", C.c_int), ("reserved", C.c_int * 5)]
+    _fields_ = [("eps", C.c_double), ("m", C.c_int), ("clamp_xy", C.c_int), ("compensated", C.c_int),
+                ("reserved", C.c_int * 4)]
+
+
+def _storage(dt: torch.dtype) -> int:
+    return _ffi.MM_BF16 if dt == torch.bfloat16 else _ffi.MM_F32
 
 
 class TomoReal:
     """Radon transform via USFFT for REAL float32 objects (processing/tomo.py:17)."""
 
-    def __init__(self, n, nz, theta, *, eps: float = 1e-3, m: int | None = None, clamp_xy: bool = False):
+    def __init__(self, n, nz, theta, *, eps: float = 1e-3, m: int | None = None, clamp_xy: bool = False,
+                 compensated: bool = False):
         require_cuda()
         L = _ffi.lib()
         self.n = int(n)
@@ -43,7 +53,8 @@ class TomoReal:
         th = np.ascontiguousarray(np.asarray(theta).astype("float32"))   # tomo.py:57
         self.ntheta = len(th)
         self.theta = th
-        opts = _TomoOpts(eps=float(eps), m=int(m or 0), clamp_xy=int(bool(clamp_xy)))
+        opts = _TomoOpts(eps=float(eps), m=int(m or 0), clamp_xy=int(bool(clamp_xy)),
+                         compensated=int(bool(compensated)))
         h = C.c_void_p()
         _ffi.check(L.mm_tomo_create(self.n, self._nz, self.ntheta, th.ctypes.data_as(C.c_void_p),
                                     C.byref(opts), C.byref(h)), "mm_tomo_create")
@@ -76,29 +87,38 @@ class TomoReal:
         _ffi.check(_ffi.lib().mm_tomo_prepare_rt(self._handle(), C.c_void_p(stream_ptr())))
 
     # -- operators -------------------------------------------------------------
-    def R(self, obj):
-        """(nz, n, n) REAL float32 obj -> (ntheta, nz, n) float32 sinogram."""
-        x, kind = to_device(obj, torch.float32)
+    def R(self, obj, out_dtype=None):
+        """(nz, n, n) REAL float32 obj -> (ntheta, nz, n) float32 sinogram.
+        A bfloat16 torch tensor is read as bfloat16; the sinogram is stored
+        as ``out_dtype`` (torch.float32 or torch.bfloat16, default: the
+        input's)."""
+        bf = isinstance(obj, torch.Tensor) and obj.dtype == torch.bfloat16
+        x, kind = to_device(obj, torch.bfloat16 if bf else torch.float32)
         if x.dim() != 3 or x.shape[1] != self.n or x.shape[2] != self.n:
             raise ValueError(f"R: obj shape {tuple(x.shape)} is not (nz, {self.n}, {self.n})")
+        odt = out_dtype or x.dtype
+        if odt not in (torch.float32, torch.bfloat16):
+            raise ValueError(f"R: out_dtype {odt} is not float32 or bfloat16")
         nz = x.shape[0]
-        out = torch.empty((self.ntheta, nz, self.n), dtype=torch.float32, device=x.device)
-        _ffi.check(_ffi.lib().mm_tomo_R(self._handle(), C.c_void_p(x.data_ptr()), C.c_void_p(out.data_ptr()),
-                                        nz, C.c_void_p(stream_ptr(x.device))), "mm_tomo_R")
+        out = torch.empty((self.ntheta, nz, self.n), dtype=odt, device=x.device)
+        _ffi.check(_ffi.lib().mm_tomo_R_ex(self._handle(), C.c_void_p(x.data_ptr()), _storage(x.dtype),
+                                           C.c_void_p(out.data_ptr()), _storage(odt), nz,
+                                           C.c_void_p(stream_ptr(x.device))), "mm_tomo_R")
         return from_device(out, kind)
 
     def RT(self, data):
         """Adjoint: (ntheta, nz, n) sinogram -> (nz, n, n) object; float32 in
         gives float32 out, complex64 in gives complex64 out (tomo.py:153-188)."""
         cplx = is_complex(data)
-        dt = torch.complex64 if cplx else torch.float32
+        bf = isinstance(data, torch.Tensor) and data.dtype == torch.bfloat16
+        dt = torch.complex64 if cplx else (torch.bfloat16 if bf else torch.float32)
         y, kind = to_device(data, dt)
         if y.dim() != 3 or y.shape[0] != self.ntheta or y.shape[2] != self.n:
             raise ValueError(f"RT: sinogram shape {tuple(y.shape)} is not ({self.ntheta}, nz, {self.n})")
         nz = y.shape[1]
         out = torch.empty((nz, self.n, self.n), dtype=dt, device=y.device)
         _ffi.check(_ffi.lib().mm_tomo_RT(self._handle(), C.c_void_p(y.data_ptr()),
-                                         _ffi.MM_C64 if cplx else _ffi.MM_F32, C.c_void_p(out.data_ptr()), nz,
+                                         _ffi.MM_C64 if cplx else _storage(dt), C.c_void_p(out.data_ptr()), nz,
                                          C.c_void_p(stream_ptr(y.device))), "mm_tomo_RT")
         return from_device(out, kind)
 
