@@ -310,6 +310,56 @@ __device__ __forceinline__ void conv(float2* __restrict__ buf, const Ad& ad, con
     }
 }
 
+// Pair-coupled convolution y = IFFT(Y) with Y[k] = pair(k, X[k], X[(N-k) mod N])
+// and X = FFT(x) (both unnormalised).  The forward's last pass leaves X[k]
+// in the registers that the reversed-schedule inverse's first pass consumes;
+// the partner X[N-k] is fetched from `buf`, where every thread parks its X
+// for one round.  Same tables as conv().
+template <int N, class Ld, class Pair, class St, class Ad>
+__device__ __forceinline__ void pairconv(float2* __restrict__ buf, const Ad& ad, const Ld& ld, const Pair& pair,
+                                         const St& st, int t, const float2* __restrict__ twf,
+                                         const float2* __restrict__ twi) {
+    using F = Sched<N, false>;
+    constexpr int P = F::P;
+    using Sf = PassShape<N, false, P - 1>;
+    using Si = PassShape<N, true, 0>;
+    static_assert(Sf::RP == Si::RP && Sf::NG == Si::NG && Sf::Q == Si::Q, "fused pass shapes");
+    auto to_buf = [&](int pos, float2 v) { buf[ad(pos)] = v; };
+    auto from_buf = [&](int pos) -> float2 { return buf[ad(pos)]; };
+    float2 x[Sf::Q][Sf::RP];
+    if constexpr (P == 1) {
+        pass_load<N, false, 0, false>(x, ld, t, twf);
+    } else {
+        run<N, false, false, 0, P - 2>(buf, ad, ld, to_buf, t, twf);
+        pass_load<N, false, P - 1, false>(x, from_buf, t, twf);
+        __syncthreads();  // everyone has read the last pass's input
+    }
+#pragma unroll
+    for (int q = 0; q < Sf::Q; ++q) {
+#pragma unroll
+        for (int i = 0; i < Sf::RP; ++i) buf[ad((t + F::G * q) + i * Sf::NG)] = x[q][i];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Sf::Q; ++q) {
+        const int j = t + F::G * q;
+#pragma unroll
+        for (int i = 0; i < Sf::RP; ++i) {
+            const int k = j + i * Sf::NG;
+            x[q][i] = pair(k, x[q][i], buf[ad((N - k) & (N - 1))]);
+        }
+        reg_fft<Sf::RP, true>(x[q]);
+    }
+    __syncthreads();  // partners read before the inverse overwrites buf
+    if constexpr (P == 1) {
+        pass_store<N, false, 0>(x, st, t);
+    } else {
+        pass_store<N, true, 0>(x, to_buf, t);
+        __syncthreads();
+        run<N, true, true, 1, P - 1>(buf, ad, ld, st, t, twi);
+    }
+}
+
 // Shared-memory addressing: a row line with one pad slot per 16 entries, or
 // column lines interleaved with lanes running over CW columns.
 struct RowAddr {

@@ -4,16 +4,27 @@
 //   D(psi) = crop( IFFT2_unnorm( fker_j * FFT2( mirrorpad(psi) ) ) ),
 //   fker_j = exp(-i pi lambda z_j (fx^2 + fy^2)) / (4 n nz).
 // The chirp separates, K = Kx(fx) Ky(fy) (processing/propagation_large.py:7-13),
-// and the y and x halves commute, so D runs as two passes over HBM:
-//   y-pass  per column: mirror-pad to 2nz, FFT, *Ky/(2nz), IFFT, crop  -> mid
-//   x-pass  per row:    mirror-pad to 2n,  FFT, *Kx/(2n),  IFFT, crop  -> out
-// Each pass keeps its column/row in registers and shared memory
-// (fft_smem.cuh): 24 bytes of HBM traffic per pixel for f32 in, c64 mid,
-// f32 out.  psi = exp(-p s/beta_r) (cos p s, sin p s) (step3_propagation.py:
-// 94-103) is built in the y-pass load and |u|^2 (:105-110) in the x-pass
-// store.  The chirp phase is evaluated in FP64 and reduced mod 2 pi.
-// DT is the exact adjoint: zero-embed, FFT, *conj(K), IFFT, fold the mirrored
-// borders back onto their source pixels.
+// and the y and x halves commute, so D runs as two passes over HBM: a column
+// pass along y (length nz) and a row pass along x (length n).
+//
+// Half-length lines.  The padding repeats the edge sample (kernels.py:541-544),
+// so the 2N-point padded line is the even, half-sample-symmetric extension of
+// the N input samples, and the chirp is even in frequency (K[k] = K[2N-k]).
+// Pad -> FFT_2N -> *K -> IFFT_2N -> crop is then exactly
+// DCT-III . diag(K[0..N)) . DCT-II on the N samples, and both DCTs run on
+// N-point complex FFTs (Makhoul's reordering, IEEE TASSP 28(1), 1980):
+//   v[p] = a[sig(p)],  sig(p) = 2p (p < N/2), 2N-1-2p (p >= N/2)
+//   V = FFT_N(v)
+//   W[k] = P[k] V[k] + Q[k] V[(N-k) mod N]
+//   out[sig(p)] = IFFT_N,unnorm(W)[p]
+// with, for the chirp Kh = K/(2N) of the 2N grid and Kh' = Kh[N-k] (Kh[0]
+// at k = 0):  P[k] = Kh[k] + Kh',  Q[k] = e^{i pi k/N} (Kh[k] - Kh')
+// (Q[0] = 0).  The operator is complex symmetric, so the adjoint DT is the
+// same line transform with conj(K): no zero embedding and no border fold.
+// Per pixel: f32 in, c64 intermediate, f32 out (24 bytes of HBM traffic);
+// psi = exp(-p s/beta_r)(cos p s, sin p s) (step3_propagation.py:94-103) is
+// built in the column-pass load and |u|^2 (:105-110) in the row-pass store.
+// Chirp phases and the P/Q tables are evaluated in FP64 (phase mod 2 pi).
 #include "mm_common.cuh"
 #include "fft_smem.cuh"
 
@@ -25,17 +36,17 @@
 using mm::dev_alloc;
 using mmfft::cmul;
 using mmfft::cmulc;
-using mmfft::reg_fft;
-using mmfft::Split;
 
 struct mm_prop {
     int n = 0, nz = 0, ntheta = 0, ndist = 0;
-    float2* Kx = nullptr;   // (ndist, 2n)
-    float2* Ky = nullptr;   // (ndist, 2nz)
-    // Stockham pass twiddles of the 2n- and 2nz-point lines (fft_smem.cuh),
-    // each in a 3L-entry slot (forward schedule, then reversed at 3L/2)
-    float2* twx = nullptr;  // (3 * 2n)
-    float2* twy = nullptr;  // (3 * 2nz)
+    // per distance, P/Q line tables as float4 (P.re, P.im, Q.re, Q.im):
+    // [dist][0][k] for D, [dist][1][k] for DT
+    float4* Sx = nullptr;   // (ndist, 2, n)
+    float4* Sy = nullptr;   // (ndist, 2, nz)
+    // Stockham pass twiddles of the n- and nz-point lines (fft_smem.cuh),
+    // each in a 3N-entry slot (forward schedule, then reversed at 3N/2)
+    float2* twx = nullptr;  // (3 * n)
+    float2* twy = nullptr;  // (3 * nz)
     float2* mid = nullptr;  // (ntheta, nz, n)
     size_t ws_bytes = 0;
     mm::StageTimer tm;
@@ -43,81 +54,45 @@ struct mm_prop {
 
 namespace {
 
-// Source index of padded position t (processing/kernels.py:541-544).
-__device__ __forceinline__ int mirror_src(int t, int len) {
-    const int h = len / 2;
-    return t < h ? h - t - 1 : (t >= len + h ? 2 * len - t + h - 1 : t - h);
-}
-// The second padded position that folds onto pixel r (the first is r + len/2).
-__device__ __forceinline__ int mirror_partner(int r, int len) {
-    const int h = len / 2;
-    return r < h ? h - 1 - r : 2 * len + h - 1 - r;
+// Makhoul order: line position p holds sample sig(p).
+__device__ __forceinline__ int sig(int p, int N) { return p < N / 2 ? 2 * p : 2 * N - 1 - 2 * p; }
+
+__device__ __forceinline__ float2 pair_mix(const float4* __restrict__ S, int k, float2 a, float2 b) {
+    const float4 pq = __ldg(S + k);
+    const float2 pa = cmul(a, make_float2(pq.x, pq.y));
+    const float2 qb = cmul(b, make_float2(pq.z, pq.w));
+    return make_float2(pa.x + qb.x, pa.y + qb.y);
 }
 
 // ---------------------------------------------------------------- y-pass
-// IN: 0 complex psi, 1 real projection (psi built on load).  Block (CW, G):
-// lanes run over CW adjacent columns, threadIdx.y over the G = 2nz/16
-// threads of each column's Stockham transform (fft_smem.cuh).
-template <int L, int CW, int IN, bool ADJ>
-__global__ void __launch_bounds__(CW * stockham::Sched<L>::G, 1024 / (CW * stockham::Sched<L>::G)) k_ypass(const void* __restrict__ src,
-                                                                       float2* __restrict__ dst,
-                                                                       const float2* __restrict__ Ky,
-                                                                       const float2* __restrict__ tw, int n, int nz,
-                                                                       float s, float ib) {
-    using S = stockham::Sched<L>;
-    extern __shared__ float2 sm[];  // buf [L][CW], then staged rows [nz][CW]
-    float2* buf = sm;
-    float2* stg = sm + L * CW;
+// IN: 0 complex input, 1 real projection (psi built on load).  Block
+// (CW, G): lanes run over CW adjacent columns, threadIdx.y over the
+// G = nz/16 threads of each column's Stockham transform (fft_smem.cuh).
+template <int N, int CW, int IN>
+__global__ void __launch_bounds__(CW * stockham::Sched<N>::G, 1024 / (CW * stockham::Sched<N>::G))
+    k_ypass(const void* __restrict__ src, float2* __restrict__ dst, const float4* __restrict__ Sy,
+            const float2* __restrict__ tw, int n, float s, float ib) {
+    extern __shared__ float2 sm[];  // [rows(N)][CW]
     const int c = threadIdx.x, g = threadIdx.y;
     const int x = blockIdx.x * CW + c;
     const bool live = x < n;
-    const long plane = (long)blockIdx.y * nz * n;
-    // stage the nz source rows of this column block once (psi built here);
-    // the mirror padding then reads each of them twice from shared memory
-    for (int r = g; r < nz; r += S::G) {
-        float2 a = make_float2(0.f, 0.f);
-        if (live) {
-            const long off = plane + (long)r * n + x;
-            if (IN == 0) {
-                a = __ldg(static_cast<const float2*>(src) + off);
-            } else {
-                const float ph = __ldg(static_cast<const float*>(src) + off) * s;
-                const float at = expf(-ph * ib);
-                float sn, cs;
-                sincosf(ph, &sn, &cs);
-                a = make_float2(at * cs, at * sn);
-            }
-        }
-        stg[r * CW + c] = a;
-    }
-    __syncthreads();
+    const long plane = (long)blockIdx.y * N * n;
     const stockham::ColAddr<CW> ad{c};
-    auto ld_in = [&](int pos) -> float2 {
-        if (!ADJ) return stg[mirror_src(pos, nz) * CW + c];
-        const int r = pos - nz / 2;
-        return (r >= 0 && r < nz) ? stg[r * CW + c] : make_float2(0.f, 0.f);
+    auto ld = [&](int pos) -> float2 {
+        if (!live) return make_float2(0.f, 0.f);
+        const long off = plane + (long)sig(pos, N) * n + x;
+        if (IN == 0) return __ldg(static_cast<const float2*>(src) + off);
+        const float ph = __ldg(static_cast<const float*>(src) + off) * s;
+        const float at = expf(-ph * ib);
+        float sn, cs;
+        sincosf(ph, &sn, &cs);
+        return make_float2(at * cs, at * sn);
     };
-    auto mul = [&](int pos, float2 v) -> float2 {
-        const float2 K = __ldg(Ky + pos);
-        return ADJ ? cmulc(v, K) : cmul(v, K);
+    auto pair = [&](int k, float2 a, float2 b) { return pair_mix(Sy, k, a, b); };
+    auto st = [&](int pos, float2 v) {
+        if (live) dst[plane + (long)sig(pos, N) * n + x] = v;
     };
-    const float2* twf = tw;
-    const float2* twi = tw + 3 * L / 2;
-    if (!ADJ) {
-        auto st_out = [&](int pos, float2 v) {
-            const int r = pos - nz / 2;
-            if (live && r >= 0 && r < nz) dst[plane + (long)r * n + x] = v;
-        };
-        stockham::conv<L>(buf, ad, ld_in, mul, st_out, g, twf, twi);
-    } else {
-        auto st_b = [&](int pos, float2 v) { buf[pos * CW + c] = v; };
-        stockham::conv<L>(buf, ad, ld_in, mul, st_b, g, twf, twi);
-        __syncthreads();
-        for (int r = g; r < nz; r += S::G) {
-            const float2 a = buf[(r + nz / 2) * CW + c], b = buf[mirror_partner(r, nz) * CW + c];
-            if (live) dst[plane + (long)r * n + x] = make_float2(a.x + b.x, a.y + b.y);
-        }
-    }
+    stockham::pairconv<N>(sm, ad, ld, pair, st, g, tw, tw + 3 * N / 2);
 }
 
 // ---------------------------------------------------------------- x-pass
@@ -125,157 +100,141 @@ __global__ void __launch_bounds__(CW * stockham::Sched<L>::G, 1024 / (CW * stock
 // g = 4 (|u|^2 - d) u with d = aux, plus per-block sums of (|u|^2 - d)^2
 // in partials[blockIdx.x]; 3 (adjoint, chain through psi): dL/dp =
 // s Re(conj(g) (i - ib) psi(p)) with p = aux, psi(p) = exp(-p s ib)(cos p s,
-// sin p s), written as float.  Block (G, RPB): G = 2n/16 threads per row.
-template <int L, int RPB, int OUT, bool ADJ>
-__global__ void __launch_bounds__(RPB * stockham::Sched<L>::G, 512 / (RPB * stockham::Sched<L>::G)) k_xpass(const float2* __restrict__ src,
-                                                                        void* __restrict__ dst,
-                                                                        const float2* __restrict__ Kx,
-                                                                        const float2* __restrict__ tw, int n,
-                                                                        long rows, const float* __restrict__ aux,
-                                                                        float* __restrict__ partials, float s,
-                                                                        float ib) {
-    extern __shared__ float2 sm[];  // [RPB][L + L/16]
-    constexpr int LP = L + L / 16;
+// sin p s), written as float.  Block (G, RPB): G = n/16 threads per row.
+template <int N, int RPB, int OUT>
+__global__ void __launch_bounds__(RPB * stockham::Sched<N>::G, 512 / (RPB * stockham::Sched<N>::G))
+    k_xpass(const float2* __restrict__ src, void* __restrict__ dst, const float4* __restrict__ Sx,
+            const float2* __restrict__ tw, long rows, const float* __restrict__ aux, float* __restrict__ partials,
+            float s, float ib) {
+    extern __shared__ float2 sm[];  // [RPB][N + N/16]
+    constexpr int LP = N + N / 16;
     const int g = threadIdx.x, rr = threadIdx.y;
     const long row = (long)blockIdx.x * RPB + rr;
     const bool live = row < rows;
     const stockham::RowAddr ad{rr * LP};
-    float2* buf = sm;
-    const float2* in = src + row * n;
-    auto ld_in = [&](int pos) -> float2 {
-        int col = ADJ ? pos - n / 2 : mirror_src(pos, n);
-        if (ADJ && (col < 0 || col >= n)) return make_float2(0.f, 0.f);
-        return live ? __ldg(in + col) : make_float2(0.f, 0.f);
-    };
-    auto mul = [&](int pos, float2 v) -> float2 {
-        const float2 K = __ldg(Kx + pos);
-        return ADJ ? cmulc(v, K) : cmul(v, K);
-    };
-    const float2* twf = tw;
-    const float2* twi = tw + 3 * L / 2;
-    if (!ADJ) {
-        float lsum = 0.f;
-        auto st_out = [&](int pos, float2 v) {
-            const int c = pos - n / 2;
-            if (live && c >= 0 && c < n) {
-                if (OUT == 0) {
-                    static_cast<float2*>(dst)[row * n + c] = v;
-                } else if (OUT == 1) {
-                    static_cast<float*>(dst)[row * n + c] = v.x * v.x + v.y * v.y;
-                } else {
-                    const float r = v.x * v.x + v.y * v.y - __ldg(aux + row * n + c);
-                    lsum = fmaf(r, r, lsum);
-                    static_cast<float2*>(dst)[row * n + c] = make_float2(4.f * r * v.x, 4.f * r * v.y);
-                }
-            }
-        };
-        stockham::conv<L>(buf, ad, ld_in, mul, st_out, g, twf, twi);
-        if (OUT == 2) {  // deterministic block sum of the squared residuals
-            __syncthreads();
-            float* red = reinterpret_cast<float*>(sm);
-            for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
-            const int tid = rr * blockDim.x + g, nw = (blockDim.x * blockDim.y + 31) / 32;
-            if ((tid & 31) == 0) red[tid >> 5] = lsum;
-            __syncthreads();
-            if (tid == 0) {
-                float t = 0.f;
-                for (int w = 0; w < nw; ++w) t += red[w];
-                partials[blockIdx.x] = t;
-            }
+    const float2* in = src + row * N;
+    auto ld = [&](int pos) -> float2 { return live ? __ldg(in + sig(pos, N)) : make_float2(0.f, 0.f); };
+    auto pair = [&](int k, float2 a, float2 b) { return pair_mix(Sx, k, a, b); };
+    float lsum = 0.f;
+    auto st = [&](int pos, float2 v) {
+        if (!live) return;
+        const long o = row * N + sig(pos, N);
+        if (OUT == 0) {
+            static_cast<float2*>(dst)[o] = v;
+        } else if (OUT == 1) {
+            static_cast<float*>(dst)[o] = v.x * v.x + v.y * v.y;
+        } else if (OUT == 2) {
+            const float r = v.x * v.x + v.y * v.y - __ldg(aux + o);
+            lsum = fmaf(r, r, lsum);
+            static_cast<float2*>(dst)[o] = make_float2(4.f * r * v.x, 4.f * r * v.y);
+        } else {
+            const float ph = __ldg(aux + o) * s;
+            const float at = expf(-ph * ib);
+            float sn, cs;
+            sincosf(ph, &sn, &cs);
+            const float px = at * cs, py = at * sn;             // psi
+            const float wx = -ib * px - py, wy = px - ib * py;  // (i - ib) psi
+            static_cast<float*>(dst)[o] = s * (v.x * wx + v.y * wy);
         }
-    } else {
-        auto st_b = [&](int pos, float2 v) { buf[ad(pos)] = v; };
-        stockham::conv<L>(buf, ad, ld_in, mul, st_b, g, twf, twi);
+    };
+    stockham::pairconv<N>(sm, ad, ld, pair, st, g, tw, tw + 3 * N / 2);
+    if (OUT == 2) {  // deterministic block sum of the squared residuals
         __syncthreads();
-        for (int c = g; c < n; c += stockham::Sched<L>::G) {
-            const float2 a = buf[ad(c + n / 2)], b = buf[ad(mirror_partner(c, n))];
-            if (!live) continue;
-            const float2 gv = make_float2(a.x + b.x, a.y + b.y);
-            if (OUT == 3) {
-                const float ph = __ldg(aux + row * n + c) * s;
-                const float at = expf(-ph * ib);
-                float sn, cs;
-                sincosf(ph, &sn, &cs);
-                const float px = at * cs, py = at * sn;              // psi
-                const float wx = -ib * px - py, wy = px - ib * py;   // (i - ib) psi
-                static_cast<float*>(dst)[row * n + c] = s * (gv.x * wx + gv.y * wy);
-            } else {
-                static_cast<float2*>(dst)[row * n + c] = gv;
-            }
+        float* red = reinterpret_cast<float*>(sm);
+        for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+        const int tid = rr * blockDim.x + g, nw = (blockDim.x * blockDim.y + 31) / 32;
+        if ((tid & 31) == 0) red[tid >> 5] = lsum;
+        __syncthreads();
+        if (tid == 0) {
+            float t = 0.f;
+            for (int w = 0; w < nw; ++w) t += red[w];
+            partials[blockIdx.x] = t;
         }
     }
 }
 
 // ---------------------------------------------------------------- launch
-template <int L, int IN, bool ADJ>
-int launch_y(mm_prop* h, const void* src, int ntheta, int j, float s, float ib, cudaStream_t st) {
-    constexpr int G = stockham::Sched<L>::G;
-    constexpr int CW0 = 256 / G;
-    constexpr int CW = CW0 < 4 ? 4 : (CW0 > 32 ? 32 : CW0);
-    const size_t smem = (size_t)(L * CW + (L / 2) * CW) * sizeof(float2);
-    auto kern = k_ypass<L, CW, IN, ADJ>;
+template <int N>
+constexpr int y_cols() {
+    constexpr int G = stockham::Sched<N>::G;
+    return 256 / G < 4 ? 4 : (256 / G > 32 ? 32 : 256 / G);
+}
+template <int N>
+constexpr int x_rows() {
+    constexpr int G = stockham::Sched<N>::G;
+    return G >= 256 ? 1 : 256 / G;
+}
+
+template <int N, int IN>
+int launch_y(mm_prop* h, const void* src, int ntheta, const float4* S, float s, float ib, cudaStream_t st) {
+    constexpr int G = stockham::Sched<N>::G;
+    constexpr int CW = y_cols<N>();
+    const size_t smem = (size_t)stockham::ColAddr<CW>::rows(N) * CW * sizeof(float2);
+    auto kern = k_ypass<N, CW, IN>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 block(CW, G), grid((h->n + CW - 1) / CW, ntheta);
     h->tm.begin(0, st);
-    kern<<<grid, block, smem, st>>>(src, h->mid, h->Ky + (size_t)j * 2 * h->nz, h->twy, h->n, h->nz, s, ib);
+    kern<<<grid, block, smem, st>>>(src, h->mid, S, h->twy, h->n, s, ib);
     MM_LAUNCHED();
     h->tm.end(st, 1);
     return MM_OK;
 }
 
-template <int L, int OUT, bool ADJ>
-int launch_x(mm_prop* h, void* dst, int ntheta, int j, cudaStream_t st, const float* aux = nullptr,
+template <int N, int OUT>
+int launch_x(mm_prop* h, void* dst, int ntheta, const float4* S, cudaStream_t st, const float* aux = nullptr,
              float* partials = nullptr, float s = 0.f, float ib = 0.f) {
-    constexpr int G = stockham::Sched<L>::G;
-    constexpr int RPB = G >= 256 ? 1 : 256 / G;
-    const size_t smem = (size_t)RPB * (L + L / 16) * sizeof(float2);
-    auto kern = k_xpass<L, RPB, OUT, ADJ>;
+    constexpr int G = stockham::Sched<N>::G;
+    constexpr int RPB = x_rows<N>();
+    const size_t smem = (size_t)RPB * (N + N / 16) * sizeof(float2);
+    auto kern = k_xpass<N, RPB, OUT>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long rows = (long)ntheta * h->nz;
     dim3 block(G, RPB), grid((unsigned)((rows + RPB - 1) / RPB));
     h->tm.begin(1, st);
-    kern<<<grid, block, smem, st>>>(h->mid, dst, h->Kx + (size_t)j * 2 * h->n, h->twx, h->n, rows, aux, partials,
-                                    s, ib);
+    kern<<<grid, block, smem, st>>>(h->mid, dst, S, h->twx, rows, aux, partials, s, ib);
     MM_LAUNCHED();
     h->tm.end(st, 1);
     return MM_OK;
 }
 
-template <int IN, bool ADJ>
-int dispatch_y(mm_prop* h, const void* src, int ntheta, int j, float s, float ib, cudaStream_t st) {
-    switch (2 * h->nz) {
-        case 4: return launch_y<4, IN, ADJ>(h, src, ntheta, j, s, ib, st);
-        case 8: return launch_y<8, IN, ADJ>(h, src, ntheta, j, s, ib, st);
-        case 16: return launch_y<16, IN, ADJ>(h, src, ntheta, j, s, ib, st);
-        case 32: return launch_y<32, IN, ADJ>(h, src, ntheta, j, s, ib, st);
-        case 64: return launch_y<64, IN, ADJ>(h, src, ntheta, j, s, ib, st);
-        case 128: return launch_y<128, IN, ADJ>(h, src, ntheta, j, s, ib, st);
-        case 256: return launch_y<256, IN, ADJ>(h, src, ntheta, j, s, ib, st);
-        case 512: return launch_y<512, IN, ADJ>(h, src, ntheta, j, s, ib, st);
-        case 1024: return launch_y<1024, IN, ADJ>(h, src, ntheta, j, s, ib, st);
-        case 2048: return launch_y<2048, IN, ADJ>(h, src, ntheta, j, s, ib, st);
-        case 4096: return launch_y<4096, IN, ADJ>(h, src, ntheta, j, s, ib, st);
+// Column pass of distance j; adj selects the conj(K) tables.
+template <int IN>
+int dispatch_y(mm_prop* h, const void* src, int ntheta, int j, bool adj, float s, float ib, cudaStream_t st) {
+    const float4* S = h->Sy + ((size_t)j * 2 + (adj ? 1 : 0)) * h->nz;
+    switch (h->nz) {
+        case 2: return launch_y<2, IN>(h, src, ntheta, S, s, ib, st);
+        case 4: return launch_y<4, IN>(h, src, ntheta, S, s, ib, st);
+        case 8: return launch_y<8, IN>(h, src, ntheta, S, s, ib, st);
+        case 16: return launch_y<16, IN>(h, src, ntheta, S, s, ib, st);
+        case 32: return launch_y<32, IN>(h, src, ntheta, S, s, ib, st);
+        case 64: return launch_y<64, IN>(h, src, ntheta, S, s, ib, st);
+        case 128: return launch_y<128, IN>(h, src, ntheta, S, s, ib, st);
+        case 256: return launch_y<256, IN>(h, src, ntheta, S, s, ib, st);
+        case 512: return launch_y<512, IN>(h, src, ntheta, S, s, ib, st);
+        case 1024: return launch_y<1024, IN>(h, src, ntheta, S, s, ib, st);
+        case 2048: return launch_y<2048, IN>(h, src, ntheta, S, s, ib, st);
     }
-    MM_REQUIRE(false, "unsupported 2*nz=%d", 2 * h->nz);
+    MM_REQUIRE(false, "unsupported nz=%d", h->nz);
 }
 
-template <int OUT, bool ADJ>
-int dispatch_x(mm_prop* h, void* dst, int ntheta, int j, cudaStream_t st, const float* aux = nullptr,
+template <int OUT>
+int dispatch_x(mm_prop* h, void* dst, int ntheta, int j, bool adj, cudaStream_t st, const float* aux = nullptr,
                float* partials = nullptr, float s = 0.f, float ib = 0.f) {
-    switch (2 * h->n) {
-        case 4: return launch_x<4, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
-        case 8: return launch_x<8, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
-        case 16: return launch_x<16, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
-        case 32: return launch_x<32, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
-        case 64: return launch_x<64, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
-        case 128: return launch_x<128, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
-        case 256: return launch_x<256, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
-        case 512: return launch_x<512, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
-        case 1024: return launch_x<1024, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
-        case 2048: return launch_x<2048, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
-        case 4096: return launch_x<4096, OUT, ADJ>(h, dst, ntheta, j, st, aux, partials, s, ib);
+    const float4* S = h->Sx + ((size_t)j * 2 + (adj ? 1 : 0)) * h->n;
+    switch (h->n) {
+        case 2: return launch_x<2, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 4: return launch_x<4, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 8: return launch_x<8, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 16: return launch_x<16, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 32: return launch_x<32, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 64: return launch_x<64, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 128: return launch_x<128, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 256: return launch_x<256, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 512: return launch_x<512, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 1024: return launch_x<1024, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 2048: return launch_x<2048, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
     }
-    MM_REQUIRE(false, "unsupported 2*n=%d", 2 * h->n);
+    MM_REQUIRE(false, "unsupported n=%d", h->n);
 }
 
 int check_call(const mm_prop* h, const void* a, const void* b, int ntheta, int j, const char* who) {
@@ -288,22 +247,38 @@ int check_call(const mm_prop* h, const void* a, const void* b, int ntheta, int j
 
 void destroy(mm_prop* h) {
     h->tm.release();
-    void* bufs[] = {h->Kx, h->Ky, h->twx, h->twy, h->mid};
+    void* bufs[] = {h->Sx, h->Sy, h->twx, h->twy, h->mid};
     for (void* b : bufs)
         if (b) cudaFree(b);
     delete h;
 }
 
-// exp(-i pi lambda z f^2) / len for the float32 fftfreq grid of `len` points
-// (processing/propagation.py:23-31), phase in FP64 reduced mod 2 pi.
-void chirp(std::vector<float2>& out, int len, double voxelsize, double wavelength, double z) {
-    const double val = 1.0 / (len * voxelsize);
-    for (int k = 0; k < len; ++k) {
-        const int kk = k < (len + 1) / 2 ? k : k - len;
-        const double f = (double)(float)(kk * val);
-        double ph = fmod(M_PI * wavelength * z * f * f, 2.0 * M_PI);
-        out[k] = make_float2((float)(cos(-ph) / len), (float)(sin(-ph) / len));
+// P/Q entry k of an N-point line (see the top of this file) for distance z:
+// the chirp exp(-i pi lambda z f^2) / (2N) on the float32 fftfreq grid of the
+// 2N padded points (processing/propagation.py:23-31), phases in FP64 reduced
+// mod 2 pi.  Host and device (allocation-free path) share this code.
+__host__ __device__ inline void chirp_2n(int k, int N, double voxelsize, double wavelength, double z, double* re,
+                                          double* im) {
+    const int L = 2 * N;
+    const double val = 1.0 / (L * voxelsize);
+    const int kk = k < (L + 1) / 2 ? k : k - L;
+    const double f = (double)(float)(kk * val);
+    const double ph = fmod(M_PI * wavelength * z * f * f, 2.0 * M_PI);
+    *re = cos(-ph) / L;
+    *im = sin(-ph) / L;
+}
+__host__ __device__ inline float4 pq_entry(int k, int N, double voxelsize, double wavelength, double z, bool adj) {
+    double ar, ai, br, bi;
+    chirp_2n(k, N, voxelsize, wavelength, z, &ar, &ai);
+    chirp_2n(k == 0 ? 0 : N - k, N, voxelsize, wavelength, z, &br, &bi);
+    if (adj) {
+        ai = -ai;
+        bi = -bi;
     }
+    const double pr = ar + br, pi = ai + bi, dr = ar - br, di = ai - bi;
+    const double c = cos(M_PI * k / N), s = sin(M_PI * k / N);
+    const double qr = k == 0 ? 0.0 : c * dr - s * di, qi = k == 0 ? 0.0 : c * di + s * dr;
+    return make_float4((float)pr, (float)pi, (float)qr, (float)qi);
 }
 
 // Stockham twiddle tables of a length-len line (fft_smem.cuh) in a 3*len
@@ -320,10 +295,9 @@ extern "C" int mm_prop_create(int n, int nz, int ntheta, int ndist, double wavel
                               const double* distance_host, mm_prop** out) {
     MM_REQUIRE(out != nullptr, "mm_prop_create: out is NULL");
     *out = nullptr;
-    MM_REQUIRE(mm_is_pow2(2L * n) && 2 * n >= 4 && 2 * n <= 4096,
-               "mm_prop_create: 2n=%d must be a power of two in [4, 4096]", 2 * n);
-    MM_REQUIRE(mm_is_pow2(2L * nz) && 2 * nz >= 4 && 2 * nz <= 4096,
-               "mm_prop_create: 2nz=%d must be a power of two in [4, 4096]", 2 * nz);
+    MM_REQUIRE(mm_is_pow2(n) && n >= 2 && n <= 2048, "mm_prop_create: n=%d must be a power of two in [2, 2048]", n);
+    MM_REQUIRE(mm_is_pow2(nz) && nz >= 2 && nz <= 2048, "mm_prop_create: nz=%d must be a power of two in [2, 2048]",
+               nz);
     MM_REQUIRE(ntheta >= 1 && ndist >= 1 && distance_host != nullptr, "mm_prop_create: bad ntheta/ndist");
     MM_REQUIRE(voxelsize > 0, "mm_prop_create: voxelsize must be positive");
     MM_CUDA(mmfft::init_constants());
@@ -332,27 +306,30 @@ extern "C" int mm_prop_create(int n, int nz, int ntheta, int ndist, double wavel
     h->nz = nz;
     h->ntheta = ntheta;
     h->ndist = ndist;
-    std::vector<float2> kx((size_t)ndist * 2 * n), ky((size_t)ndist * 2 * nz), tx, ty, tmp;
-    for (int j = 0; j < ndist; ++j) {
-        tmp.assign(2 * n, make_float2(0, 0));
-        chirp(tmp, 2 * n, voxelsize, wavelength, distance_host[j]);
-        std::copy(tmp.begin(), tmp.end(), kx.begin() + (size_t)j * 2 * n);
-        tmp.assign(2 * nz, make_float2(0, 0));
-        chirp(tmp, 2 * nz, voxelsize, wavelength, distance_host[j]);
-        std::copy(tmp.begin(), tmp.end(), ky.begin() + (size_t)j * 2 * nz);
-    }
-    twiddles(tx, 2 * n);
-    twiddles(ty, 2 * nz);
-    struct B { float2** p; const std::vector<float2>* v; const char* what; } bs[] = {
-        {&h->Kx, &kx, "x chirp"}, {&h->Ky, &ky, "y chirp"}, {&h->twx, &tx, "x twiddles"}, {&h->twy, &ty, "y twiddles"}};
+    std::vector<float4> sx((size_t)ndist * 2 * n), sy((size_t)ndist * 2 * nz);
+    std::vector<float2> tx, ty;
+    for (int j = 0; j < ndist; ++j)
+        for (int a = 0; a < 2; ++a) {
+            for (int k = 0; k < n; ++k)
+                sx[((size_t)j * 2 + a) * n + k] = pq_entry(k, n, voxelsize, wavelength, distance_host[j], a == 1);
+            for (int k = 0; k < nz; ++k)
+                sy[((size_t)j * 2 + a) * nz + k] = pq_entry(k, nz, voxelsize, wavelength, distance_host[j], a == 1);
+        }
+    twiddles(tx, n);
+    twiddles(ty, nz);
+    struct B { void** p; const void* v; size_t bytes; const char* what; } bs[] = {
+        {(void**)&h->Sx, sx.data(), sx.size() * sizeof(float4), "x line tables"},
+        {(void**)&h->Sy, sy.data(), sy.size() * sizeof(float4), "y line tables"},
+        {(void**)&h->twx, tx.data(), tx.size() * sizeof(float2), "x twiddles"},
+        {(void**)&h->twy, ty.data(), ty.size() * sizeof(float2), "y twiddles"}};
     for (auto& b : bs) {
-        int rc = dev_alloc((void**)b.p, b.v->size() * sizeof(float2), b.what);
+        int rc = dev_alloc(b.p, b.bytes, b.what);
         if (rc != MM_OK) {
             destroy(h);
             return rc;
         }
-        h->ws_bytes += b.v->size() * sizeof(float2);
-        if (cudaMemcpy(*b.p, b.v->data(), b.v->size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess) {
+        h->ws_bytes += b.bytes;
+        if (cudaMemcpy(*b.p, b.v, b.bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
             mm::set_error("mm_prop_create: table upload failed");
             destroy(h);
             return MM_ECUDA;
@@ -379,23 +356,23 @@ extern "C" int mm_prop_destroy(mm_prop* h) {
 extern "C" int mm_prop_D(mm_prop* h, const void* psi, void* out, int ntheta, int j, void* stream) {
     MM_TRY(check_call(h, psi, out, ntheta, j, "mm_prop_D"));
     cudaStream_t st = (cudaStream_t)stream;
-    MM_TRY((dispatch_y<0, false>(h, psi, ntheta, j, 0.f, 0.f, st)));
-    return dispatch_x<0, false>(h, out, ntheta, j, st);
+    MM_TRY((dispatch_y<0>(h, psi, ntheta, j, false, 0.f, 0.f, st)));
+    return dispatch_x<0>(h, out, ntheta, j, false, st);
 }
 
 extern "C" int mm_prop_DT(mm_prop* h, const void* g, void* out, int ntheta, int j, void* stream) {
     MM_TRY(check_call(h, g, out, ntheta, j, "mm_prop_DT"));
     cudaStream_t st = (cudaStream_t)stream;
-    MM_TRY((dispatch_y<0, true>(h, g, ntheta, j, 0.f, 0.f, st)));
-    return dispatch_x<0, true>(h, out, ntheta, j, st);
+    MM_TRY((dispatch_y<0>(h, g, ntheta, j, true, 0.f, 0.f, st)));
+    return dispatch_x<0>(h, out, ntheta, j, true, st);
 }
 
 extern "C" int mm_prop_intensity(mm_prop* h, const float* proj, float inv_norm, float inv_beta_ratio,
                                  float* intensity, int ntheta, int j, void* stream) {
     MM_TRY(check_call(h, proj, intensity, ntheta, j, "mm_prop_intensity"));
     cudaStream_t st = (cudaStream_t)stream;
-    MM_TRY((dispatch_y<1, false>(h, proj, ntheta, j, inv_norm, inv_beta_ratio, st)));
-    return dispatch_x<1, false>(h, intensity, ntheta, j, st);
+    MM_TRY((dispatch_y<1>(h, proj, ntheta, j, false, inv_norm, inv_beta_ratio, st)));
+    return dispatch_x<1>(h, intensity, ntheta, j, false, st);
 }
 
 extern "C" int mm_prop_set_timing(mm_prop* h, int on) {
@@ -461,30 +438,26 @@ int noalloc_setup(float2** out) {
     return MM_OK;
 }
 
-// Chirp and twiddle tables of one distance, computed on the device in FP64
-// exactly as chirp() / twiddles() do on the host for mm_prop_create.
-__global__ void k_noalloc_tables(float2* __restrict__ Kx, float2* __restrict__ Ky, float2* __restrict__ twx,
+// Line and twiddle tables of one distance, computed on the device in FP64
+// exactly as pq_entry() / twiddles() do on the host for mm_prop_create.
+__global__ void k_noalloc_tables(float4* __restrict__ Sx, float4* __restrict__ Sy, float2* __restrict__ twx,
                                  float2* __restrict__ twy, int n, int nz, double wavelength, double voxelsize,
                                  double z) {
-    const int total = 2 * n + 2 * nz + 6 * n + 6 * nz;
+    const int total = n + nz + 3 * n + 3 * nz;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         int i = t;
-        if (i < 2 * n + 2 * nz) {  // chirp along x then y
-            const bool along_x = i < 2 * n;
-            const int len = along_x ? 2 * n : 2 * nz;
-            const int k = along_x ? i : i - 2 * n;
-            const double val = 1.0 / (len * voxelsize);
-            const int kk = k < (len + 1) / 2 ? k : k - len;
-            const double f = (double)(float)(kk * val);
-            const double ph = fmod(M_PI * wavelength * z * f * f, 2.0 * M_PI);
-            const float2 w = make_float2((float)(cos(-ph) / len), (float)(sin(-ph) / len));
-            if (along_x) Kx[k] = w; else Ky[k] = w;
+        if (i < n + nz) {  // P/Q along x then y
+            const bool along_x = i < n;
+            const int N = along_x ? n : nz;
+            const int k = along_x ? i : i - n;
+            const float4 e = pq_entry(k, N, voxelsize, wavelength, z, false);
+            if (along_x) Sx[k] = e; else Sy[k] = e;
             continue;
         }
-        i -= 2 * n + 2 * nz;  // twiddles: x slot (3 * 2n) then y slot (3 * 2nz)
-        const bool along_x = i < 6 * n;
-        const int len = along_x ? 2 * n : 2 * nz;
-        int q = along_x ? i : i - 6 * n;
+        i -= n + nz;  // twiddles: x slot (3n) then y slot (3nz)
+        const bool along_x = i < 3 * n;
+        const int len = along_x ? n : nz;
+        int q = along_x ? i : i - 3 * n;
         float2* tab = along_x ? twx : twy;
         const int slot_q = q;
         const bool rev = q >= 3 * len / 2;
@@ -519,10 +492,10 @@ __global__ void k_noalloc_tables(float2* __restrict__ Kx, float2* __restrict__ K
 extern "C" int mm_prop_D_noalloc(int n, int nz, int ntheta, double wavelength, double voxelsize, double distance,
                                  const void* psi, void* out, void* stream) {
     MM_REQUIRE(psi != nullptr && out != nullptr, "mm_prop_D_noalloc: NULL array");
-    MM_REQUIRE(mm_is_pow2(2L * n) && 2 * n >= 4 && 2 * n <= 4096,
-               "mm_prop_D_noalloc: 2n=%d must be a power of two in [4, 4096]", 2 * n);
-    MM_REQUIRE(mm_is_pow2(2L * nz) && 2 * nz >= 4 && 2 * nz <= 4096,
-               "mm_prop_D_noalloc: 2nz=%d must be a power of two in [4, 4096]", 2 * nz);
+    MM_REQUIRE(mm_is_pow2(n) && n >= 2 && n <= 2048, "mm_prop_D_noalloc: n=%d must be a power of two in [2, 2048]",
+               n);
+    MM_REQUIRE(mm_is_pow2(nz) && nz >= 2 && nz <= 2048,
+               "mm_prop_D_noalloc: nz=%d must be a power of two in [2, 2048]", nz);
     MM_REQUIRE(ntheta >= 1 && voxelsize > 0, "mm_prop_D_noalloc: bad ntheta/voxelsize");
     const size_t tables = (size_t)8 * n + 8 * nz;
     const size_t need = (tables + (size_t)ntheta * nz * n) * sizeof(float2);
@@ -538,21 +511,22 @@ extern "C" int mm_prop_D_noalloc(int n, int nz, int ntheta, double wavelength, d
     h.nz = nz;
     h.ntheta = ntheta;
     h.ndist = 1;
-    h.Kx = base;
-    h.Ky = h.Kx + 2 * n;
-    h.twx = h.Ky + 2 * nz;
-    h.twy = h.twx + 6 * n;
-    h.mid = h.twy + 6 * nz;
-    k_noalloc_tables<<<(unsigned)((tables + 255) / 256), 256, 0, st>>>(h.Kx, h.Ky, h.twx, h.twy, n, nz, wavelength,
+    // float2 slots: Sx (n float4) | Sy (nz float4) | twx (3n) | twy (3nz) | ... | mid at 8(n + nz)
+    h.Sx = reinterpret_cast<float4*>(base);
+    h.Sy = reinterpret_cast<float4*>(base + 2 * n);
+    h.twx = base + 2 * n + 2 * nz;
+    h.twy = h.twx + 3 * n;
+    h.mid = base + tables;
+    k_noalloc_tables<<<(unsigned)((tables + 255) / 256), 256, 0, st>>>(h.Sx, h.Sy, h.twx, h.twy, n, nz, wavelength,
                                                                       voxelsize, distance);
     MM_LAUNCHED();
-    MM_TRY((dispatch_y<0, false>(&h, psi, ntheta, 0, 0.f, 0.f, st)));
-    return dispatch_x<0, false>(&h, out, ntheta, 0, st);
+    MM_TRY((dispatch_y<0>(&h, psi, ntheta, 0, false, 0.f, 0.f, st)));
+    return dispatch_x<0>(&h, out, ntheta, 0, false, st);
 }
 
 extern "C" long mm_prop_grad_partials(mm_prop* h, int ntheta) {
     if (!h || ntheta < 1) return 0;
-    const int G = (2 * h->n) >= 16 ? (2 * h->n) / 16 : 1;
+    const int G = h->n >= 16 ? h->n / 16 : 1;
     const int rpb = G >= 256 ? 1 : 256 / G;
     return ((long)ntheta * h->nz + rpb - 1) / rpb;
 }
@@ -563,8 +537,8 @@ extern "C" int mm_prop_grad_forward(mm_prop* h, const float* proj, const float* 
     MM_TRY(check_call(h, proj, gu, ntheta, j, "mm_prop_grad_forward"));
     MM_REQUIRE(data != nullptr && partials != nullptr, "mm_prop_grad_forward: NULL data/partials");
     cudaStream_t st = (cudaStream_t)stream;
-    MM_TRY((dispatch_y<1, false>(h, proj, ntheta, j, inv_norm, inv_beta_ratio, st)));
-    return dispatch_x<2, false>(h, gu, ntheta, j, st, data, partials, inv_norm, inv_beta_ratio);
+    MM_TRY((dispatch_y<1>(h, proj, ntheta, j, false, inv_norm, inv_beta_ratio, st)));
+    return dispatch_x<2>(h, gu, ntheta, j, false, st, data, partials, inv_norm, inv_beta_ratio);
 }
 
 extern "C" int mm_prop_grad_backward(mm_prop* h, const void* gu, const float* proj, float inv_norm,
@@ -572,6 +546,6 @@ extern "C" int mm_prop_grad_backward(mm_prop* h, const void* gu, const float* pr
     MM_TRY(check_call(h, gu, gp, ntheta, j, "mm_prop_grad_backward"));
     MM_REQUIRE(proj != nullptr, "mm_prop_grad_backward: NULL proj");
     cudaStream_t st = (cudaStream_t)stream;
-    MM_TRY((dispatch_y<0, true>(h, gu, ntheta, j, 0.f, 0.f, st)));
-    return dispatch_x<3, true>(h, gp, ntheta, j, st, proj, nullptr, inv_norm, inv_beta_ratio);
+    MM_TRY((dispatch_y<0>(h, gu, ntheta, j, true, 0.f, 0.f, st)));
+    return dispatch_x<3>(h, gp, ntheta, j, true, st, proj, nullptr, inv_norm, inv_beta_ratio);
 }
