@@ -66,9 +66,10 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic(kernel):
-    """Per-launch DRAM bytes of `kernel` from a committed ncu summary, if any:
-    a line 'traffic_bytes_per_launch <kernel> <bytes>' in profiles/*.md."""
+def profile_traffic(workload, kernel):
+    """Per-launch DRAM bytes of `kernel` on `workload` from a committed ncu
+    summary, if any: a line 'traffic_bytes_per_launch <workload> <kernel>
+    <bytes>' in profiles/*.md."""
     pdir = os.path.join(ROOT, "profiles")
     if not os.path.isdir(pdir):
         return None
@@ -77,8 +78,9 @@ def profile_traffic(kernel):
             continue
         for line in open(os.path.join(pdir, fn)):
             parts = line.strip().strip("`").split()
-            if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == kernel:
-                return float(parts[2])
+            if (len(parts) == 4 and parts[0] == "traffic_bytes_per_launch" and parts[1] == workload
+                    and parts[2] == kernel):
+                return float(parts[3])
     return None
 
 
@@ -247,23 +249,23 @@ def run_ours(args, w, rank, world, local_rank):
     P = T * nz * n
     H = 2 * n * (n + 1) * nz
     Kh = n // 2 + 1
-    alg = {  # algorithmic bytes per launch
-        "gather": 8 * H + 8 * Kh * T * nz,
-        "pad_phi": 4 * V + 8 * V,
-        "transpose_in": 2 * 8 * nz * n * (n + 1),
-        "y_pass": 4 * P + 8 * P,
-        "x_pass": 8 * P + 4 * P,
+    alg = {  # algorithmic bytes per launch: each kernel's inputs read once, outputs written once
+        "pad_phi": 4 * V + 8 * nz * n * (n + 1),               # k_xfwd: obj -> centre rows of Y
+        "y_fft": 8 * nz * n * (n + 1) + 16 * nz * n * (n + 1),  # k_col_fft: centre rows -> 2n rows
+        "gather": 8 * H + 8 * Kh * T * nz,                     # k_gather: half spectrum -> polar lines
+        "r_c2r": 8 * Kh * T * nz + 4 * T * nz * n,             # k_rc2r: polar lines -> sinogram
+        "y_pass": 4 * P + 8 * P,                               # k_ypass: p -> psi -> column pass
+        "x_pass": 8 * P + 4 * P,                               # k_xpass: row pass -> |.|^2
     }
-    own = {"gather": tstages["gather"], "pad_phi": tstages["pad_phi"],
-           "transpose_in": tstages["transpose_in"], "y_pass": pstages["y_pass"], "x_pass": pstages["x_pass"]}
+    own = {k: (tstages if k in tstages else pstages)[k] for k in alg if k in tstages or k in pstages}
     top = max(own, key=lambda k: own[k][0])
     t_launch = own[top][0] / max(1, own[top][1])
     peak, peak_kind = peaks()
     achieved = alg[top] / (t_launch * 1e-3) / 1e9
-    kname = {"gather": "k_gather", "pad_phi": "k_pad_phi", "transpose_in": "k_transpose_in",
+    kname = {"gather": "k_gather", "pad_phi": "k_xfwd", "y_fft": "k_col_fft", "r_c2r": "k_rc2r",
              "y_pass": "k_ypass", "x_pass": "k_xpass"}[top]
-    traffic = profile_traffic(kname)
-    step_bytes = sum(alg.values()) - alg["pad_phi"] - alg["transpose_in"]    # B_R-like + B_D
+    traffic = profile_traffic(args.workload, kname)
+    step_bytes = sum(alg.values())
     roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak,
             "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "traffic": traffic, "alg_bytes_per_launch": alg[top], "ms_per_launch": round(t_launch, 4)}
