@@ -100,7 +100,9 @@ int mm_tomo_get_timing(mm_tomo* h, double* ms, long long* calls, int nstages, lo
  * mm_prop_create replaces Propagation.__init__(n, nz, ntheta, ndist,
  *   wavelength, voxelsize, distance) (processing/propagation.py:18-35) and
  *   PropagationLarge.__init__ (processing/propagation_large.py:55-94).
- *   n and nz must be powers of two in [2, 2048]. */
+ *   Any n, nz in [2, 16384]: powers of two up to 2048 run the fused
+ *   two-pass kernels, other sizes the general path (cuFFT 2-D transforms
+ *   between reordering kernels). */
 int mm_prop_create(int n, int nz, int ntheta, int ndist, double wavelength,
                    double voxelsize, const double* distance_host, mm_prop** out);
 int mm_prop_destroy(mm_prop* h);

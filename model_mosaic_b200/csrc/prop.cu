@@ -25,11 +25,19 @@
 // psi = exp(-p s/beta_r)(cos p s, sin p s) (step3_propagation.py:94-103) is
 // built in the column-pass load and |u|^2 (:105-110) in the row-pass store.
 // Chirp phases and the P/Q tables are evaluated in FP64 (phase mod 2 pi).
+//
+// General sizes.  The identity holds for every N (with the split point of
+// sig at ceil(N/2)), so sizes outside the fused kernels' range (n or nz not a
+// power of two in [2, 2048]) run the same algebra in 2-D: a reordering load
+// (psi on load), one cuFFT 2-D transform per frame, the tensor-product pair
+// step W = (Py + Qy Ry)(Px + Qx Rx) V with R the reflection k -> N-k, the
+// inverse transform and a reordering store (|.|^2 or the loss terms).
 #include "mm_common.cuh"
 #include "fft_smem.cuh"
 
 #include <math.h>
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -48,6 +56,12 @@ struct mm_prop {
     float2* twx = nullptr;  // (3 * n)
     float2* twy = nullptr;  // (3 * nz)
     float2* mid = nullptr;  // (ntheta, nz, n)
+    // general sizes: second frame buffer and cuFFT 2-D plans (ntheta frames,
+    // and the last smaller batch used)
+    bool general = false;
+    float2* mid2 = nullptr;
+    cufftHandle plan_full = 0, plan_part = 0;
+    int part_batch = 0;
     size_t ws_bytes = 0;
     mm::StageTimer tm;
 };
@@ -55,7 +69,7 @@ struct mm_prop {
 namespace {
 
 // Makhoul order: line position p holds sample sig(p).
-__device__ __forceinline__ int sig(int p, int N) { return p < N / 2 ? 2 * p : 2 * N - 1 - 2 * p; }
+__device__ __forceinline__ int sig(int p, int N) { return p < (N + 1) / 2 ? 2 * p : 2 * N - 1 - 2 * p; }
 
 __device__ __forceinline__ float2 pair_mix(const float4* __restrict__ S, int k, float2 a, float2 b) {
     const float4 pq = __ldg(S + k);
@@ -153,6 +167,94 @@ __global__ void __launch_bounds__(RPB * stockham::Sched<N>::G, 512 / (RPB * stoc
     }
 }
 
+// ---------------------------------------------------------------- general sizes
+// v[t][p][q] = a[t][sig(p)][sig(q)] (IN 0: complex a; IN 1: a = psi(p s)).
+template <int IN>
+__global__ void k_gen_load(const void* __restrict__ src, float2* __restrict__ v, long total, int nz, int n, float s,
+                           float ib) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int q = (int)(i % n);
+        const long r = i / n;
+        const int p = (int)(r % nz);
+        const long t = r / nz;
+        const long o = (t * nz + sig(p, nz)) * n + sig(q, n);
+        if (IN == 0) {
+            v[i] = __ldg(static_cast<const float2*>(src) + o);
+        } else {
+            const float ph = __ldg(static_cast<const float*>(src) + o) * s;
+            const float at = expf(-ph * ib);
+            float sn, cs;
+            sincosf(ph, &sn, &cs);
+            v[i] = make_float2(at * cs, at * sn);
+        }
+    }
+}
+
+// W[k][l] = sum over the four reflections of V (y and x pair tables).
+__global__ void k_gen_mix(const float2* __restrict__ V, float2* __restrict__ W, const float4* __restrict__ Sy,
+                          const float4* __restrict__ Sx, long total, int nz, int n) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int l = (int)(i % n);
+        const long r = i / n;
+        const int k = (int)(r % nz);
+        const float2* fr = V + (r / nz) * nz * n;
+        const int kr = k == 0 ? 0 : nz - k, lr = l == 0 ? 0 : n - l;
+        const float4 y = __ldg(Sy + k), x = __ldg(Sx + l);
+        const float2 py = make_float2(y.x, y.y), qy = make_float2(y.z, y.w);
+        const float2 px = make_float2(x.x, x.y), qx = make_float2(x.z, x.w);
+        const float2 a = cmul(__ldg(fr + (long)k * n + l), px);
+        const float2 b = cmul(__ldg(fr + (long)k * n + lr), qx);
+        const float2 c = cmul(__ldg(fr + (long)kr * n + l), px);
+        const float2 d = cmul(__ldg(fr + (long)kr * n + lr), qx);
+        const float2 ab = cmul(make_float2(a.x + b.x, a.y + b.y), py);
+        const float2 cd = cmul(make_float2(c.x + d.x, c.y + d.y), qy);
+        W[i] = make_float2(ab.x + cd.x, ab.y + cd.y);
+    }
+}
+
+// out[t][sig(p)][sig(q)] from w[t][p][q]; one block per (t, p) row.  OUT as
+// in k_xpass; OUT 2 writes one partial per row.
+template <int OUT>
+__global__ void k_gen_store(const float2* __restrict__ w, void* __restrict__ dst, int nz, int n,
+                            const float* __restrict__ aux, float* __restrict__ partials, float s, float ib) {
+    __shared__ float red[32];
+    const long row = blockIdx.x;  // t * nz + p
+    const int p = (int)(row % nz);
+    const long orow = (row - p + sig(p, nz)) * n;
+    float lsum = 0.f;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        const float2 v = w[row * n + q];
+        const long o = orow + sig(q, n);
+        if (OUT == 0) {
+            static_cast<float2*>(dst)[o] = v;
+        } else if (OUT == 1) {
+            static_cast<float*>(dst)[o] = v.x * v.x + v.y * v.y;
+        } else if (OUT == 2) {
+            const float r = v.x * v.x + v.y * v.y - __ldg(aux + o);
+            lsum = fmaf(r, r, lsum);
+            static_cast<float2*>(dst)[o] = make_float2(4.f * r * v.x, 4.f * r * v.y);
+        } else {
+            const float ph = __ldg(aux + o) * s;
+            const float at = expf(-ph * ib);
+            float sn, cs;
+            sincosf(ph, &sn, &cs);
+            const float px = at * cs, py = at * sn;
+            const float wx = -ib * px - py, wy = px - ib * py;
+            static_cast<float*>(dst)[o] = s * (v.x * wx + v.y * wy);
+        }
+    }
+    if (OUT == 2) {
+        for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = lsum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float t = 0.f;
+            for (int i = 0; i < (int)(blockDim.x + 31) / 32; ++i) t += red[i];
+            partials[row] = t;
+        }
+    }
+}
+
 // ---------------------------------------------------------------- launch
 template <int N>
 constexpr int y_cols() {
@@ -237,6 +339,51 @@ int dispatch_x(mm_prop* h, void* dst, int ntheta, int j, bool adj, cudaStream_t 
     MM_REQUIRE(false, "unsupported n=%d", h->n);
 }
 
+// cuFFT 2-D plan over `nt` frames of nz x n (cached: all frames, and the last
+// smaller batch).
+int gen_plan(mm_prop* h, int nt, cufftHandle* out) {
+    cufftHandle* slot = nt == h->ntheta ? &h->plan_full : &h->plan_part;
+    if (nt != h->ntheta && h->part_batch != nt && h->plan_part) {
+        cufftDestroy(h->plan_part);
+        h->plan_part = 0;
+    }
+    if (!*slot) {
+        int dims[2] = {h->nz, h->n};
+        MM_CUFFT(cufftPlanMany(slot, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, nt));
+        if (nt != h->ntheta) h->part_batch = nt;
+    }
+    *out = *slot;
+    return MM_OK;
+}
+
+// One D (adj = false) or DT (adj = true) on general sizes: IN / OUT as in
+// the fused passes.
+template <int IN, int OUT>
+int run_general(mm_prop* h, const void* src, void* dst, int nt, int j, bool adj, cudaStream_t st,
+                const float* aux = nullptr, float* partials = nullptr, float s = 0.f, float ib = 0.f) {
+    const long total = (long)nt * h->nz * h->n;
+    const int bs = 256;
+    const unsigned grid = (unsigned)std::min<long>((total + bs - 1) / bs, 148L * 16);
+    cufftHandle plan;
+    MM_TRY(gen_plan(h, nt, &plan));
+    MM_CUFFT(cufftSetStream(plan, st));
+    h->tm.begin(0, st);
+    k_gen_load<IN><<<grid, bs, 0, st>>>(src, h->mid, total, h->nz, h->n, s, ib);
+    MM_LAUNCHED();
+    MM_CUFFT(cufftExecC2C(plan, (cufftComplex*)h->mid, (cufftComplex*)h->mid2, CUFFT_FORWARD));
+    const float4* Sy = h->Sy + ((size_t)j * 2 + (adj ? 1 : 0)) * h->nz;
+    const float4* Sx = h->Sx + ((size_t)j * 2 + (adj ? 1 : 0)) * h->n;
+    k_gen_mix<<<grid, bs, 0, st>>>(h->mid2, h->mid, Sy, Sx, total, h->nz, h->n);
+    MM_LAUNCHED();
+    MM_CUFFT(cufftExecC2C(plan, (cufftComplex*)h->mid, (cufftComplex*)h->mid2, CUFFT_INVERSE));
+    h->tm.end(st, 2);
+    h->tm.begin(1, st);
+    k_gen_store<OUT><<<(unsigned)((long)nt * h->nz), 256, 0, st>>>(h->mid2, dst, h->nz, h->n, aux, partials, s, ib);
+    MM_LAUNCHED();
+    h->tm.end(st, 1);
+    return MM_OK;
+}
+
 int check_call(const mm_prop* h, const void* a, const void* b, int ntheta, int j, const char* who) {
     MM_REQUIRE(h != nullptr, "%s: NULL handle", who);
     MM_REQUIRE(a != nullptr && b != nullptr, "%s: NULL array", who);
@@ -247,7 +394,9 @@ int check_call(const mm_prop* h, const void* a, const void* b, int ntheta, int j
 
 void destroy(mm_prop* h) {
     h->tm.release();
-    void* bufs[] = {h->Sx, h->Sy, h->twx, h->twy, h->mid};
+    if (h->plan_full) cufftDestroy(h->plan_full);
+    if (h->plan_part) cufftDestroy(h->plan_part);
+    void* bufs[] = {h->Sx, h->Sy, h->twx, h->twy, h->mid, h->mid2};
     for (void* b : bufs)
         if (b) cudaFree(b);
     delete h;
@@ -295,8 +444,7 @@ extern "C" int mm_prop_create(int n, int nz, int ntheta, int ndist, double wavel
                               const double* distance_host, mm_prop** out) {
     MM_REQUIRE(out != nullptr, "mm_prop_create: out is NULL");
     *out = nullptr;
-    MM_REQUIRE(mm_is_pow2(n) && n >= 2 && n <= 2048, "mm_prop_create: n=%d must be a power of two in [2, 2048]", n);
-    MM_REQUIRE(mm_is_pow2(nz) && nz >= 2 && nz <= 2048, "mm_prop_create: nz=%d must be a power of two in [2, 2048]",
+    MM_REQUIRE(n >= 2 && n <= 16384 && nz >= 2 && nz <= 16384, "mm_prop_create: n=%d, nz=%d outside [2, 16384]", n,
                nz);
     MM_REQUIRE(ntheta >= 1 && ndist >= 1 && distance_host != nullptr, "mm_prop_create: bad ntheta/ndist");
     MM_REQUIRE(voxelsize > 0, "mm_prop_create: voxelsize must be positive");
@@ -306,6 +454,7 @@ extern "C" int mm_prop_create(int n, int nz, int ntheta, int ndist, double wavel
     h->nz = nz;
     h->ntheta = ntheta;
     h->ndist = ndist;
+    h->general = !(mm_is_pow2(n) && n <= 2048 && mm_is_pow2(nz) && nz <= 2048);
     std::vector<float4> sx((size_t)ndist * 2 * n), sy((size_t)ndist * 2 * nz);
     std::vector<float2> tx, ty;
     for (int j = 0; j < ndist; ++j)
@@ -315,14 +464,17 @@ extern "C" int mm_prop_create(int n, int nz, int ntheta, int ndist, double wavel
             for (int k = 0; k < nz; ++k)
                 sy[((size_t)j * 2 + a) * nz + k] = pq_entry(k, nz, voxelsize, wavelength, distance_host[j], a == 1);
         }
-    twiddles(tx, n);
-    twiddles(ty, nz);
+    if (!h->general) {
+        twiddles(tx, n);
+        twiddles(ty, nz);
+    }
     struct B { void** p; const void* v; size_t bytes; const char* what; } bs[] = {
         {(void**)&h->Sx, sx.data(), sx.size() * sizeof(float4), "x line tables"},
         {(void**)&h->Sy, sy.data(), sy.size() * sizeof(float4), "y line tables"},
         {(void**)&h->twx, tx.data(), tx.size() * sizeof(float2), "x twiddles"},
         {(void**)&h->twy, ty.data(), ty.size() * sizeof(float2), "y twiddles"}};
     for (auto& b : bs) {
+        if (b.bytes == 0) continue;
         int rc = dev_alloc(b.p, b.bytes, b.what);
         if (rc != MM_OK) {
             destroy(h);
@@ -337,11 +489,12 @@ extern "C" int mm_prop_create(int n, int nz, int ntheta, int ndist, double wavel
     }
     const size_t mid = (size_t)ntheta * nz * n;
     int rc = dev_alloc((void**)&h->mid, mid * sizeof(float2), "propagator intermediate");
+    if (rc == MM_OK && h->general) rc = dev_alloc((void**)&h->mid2, mid * sizeof(float2), "propagator spectrum");
     if (rc != MM_OK) {
         destroy(h);
         return rc;
     }
-    h->ws_bytes += mid * sizeof(float2);
+    h->ws_bytes += mid * sizeof(float2) * (h->general ? 2 : 1);
     *out = h;
     return MM_OK;
 }
@@ -356,6 +509,7 @@ extern "C" int mm_prop_destroy(mm_prop* h) {
 extern "C" int mm_prop_D(mm_prop* h, const void* psi, void* out, int ntheta, int j, void* stream) {
     MM_TRY(check_call(h, psi, out, ntheta, j, "mm_prop_D"));
     cudaStream_t st = (cudaStream_t)stream;
+    if (h->general) return run_general<0, 0>(h, psi, out, ntheta, j, false, st);
     MM_TRY((dispatch_y<0>(h, psi, ntheta, j, false, 0.f, 0.f, st)));
     return dispatch_x<0>(h, out, ntheta, j, false, st);
 }
@@ -363,6 +517,7 @@ extern "C" int mm_prop_D(mm_prop* h, const void* psi, void* out, int ntheta, int
 extern "C" int mm_prop_DT(mm_prop* h, const void* g, void* out, int ntheta, int j, void* stream) {
     MM_TRY(check_call(h, g, out, ntheta, j, "mm_prop_DT"));
     cudaStream_t st = (cudaStream_t)stream;
+    if (h->general) return run_general<0, 0>(h, g, out, ntheta, j, true, st);
     MM_TRY((dispatch_y<0>(h, g, ntheta, j, true, 0.f, 0.f, st)));
     return dispatch_x<0>(h, out, ntheta, j, true, st);
 }
@@ -371,6 +526,8 @@ extern "C" int mm_prop_intensity(mm_prop* h, const float* proj, float inv_norm, 
                                  float* intensity, int ntheta, int j, void* stream) {
     MM_TRY(check_call(h, proj, intensity, ntheta, j, "mm_prop_intensity"));
     cudaStream_t st = (cudaStream_t)stream;
+    if (h->general)
+        return run_general<1, 1>(h, proj, intensity, ntheta, j, false, st, nullptr, nullptr, inv_norm, inv_beta_ratio);
     MM_TRY((dispatch_y<1>(h, proj, ntheta, j, false, inv_norm, inv_beta_ratio, st)));
     return dispatch_x<1>(h, intensity, ntheta, j, false, st);
 }
@@ -526,6 +683,7 @@ extern "C" int mm_prop_D_noalloc(int n, int nz, int ntheta, double wavelength, d
 
 extern "C" long mm_prop_grad_partials(mm_prop* h, int ntheta) {
     if (!h || ntheta < 1) return 0;
+    if (h->general) return (long)ntheta * h->nz;
     const int G = h->n >= 16 ? h->n / 16 : 1;
     const int rpb = G >= 256 ? 1 : 256 / G;
     return ((long)ntheta * h->nz + rpb - 1) / rpb;
@@ -537,6 +695,8 @@ extern "C" int mm_prop_grad_forward(mm_prop* h, const float* proj, const float* 
     MM_TRY(check_call(h, proj, gu, ntheta, j, "mm_prop_grad_forward"));
     MM_REQUIRE(data != nullptr && partials != nullptr, "mm_prop_grad_forward: NULL data/partials");
     cudaStream_t st = (cudaStream_t)stream;
+    if (h->general)
+        return run_general<1, 2>(h, proj, gu, ntheta, j, false, st, data, partials, inv_norm, inv_beta_ratio);
     MM_TRY((dispatch_y<1>(h, proj, ntheta, j, false, inv_norm, inv_beta_ratio, st)));
     return dispatch_x<2>(h, gu, ntheta, j, false, st, data, partials, inv_norm, inv_beta_ratio);
 }
@@ -546,6 +706,8 @@ extern "C" int mm_prop_grad_backward(mm_prop* h, const void* gu, const float* pr
     MM_TRY(check_call(h, gu, gp, ntheta, j, "mm_prop_grad_backward"));
     MM_REQUIRE(proj != nullptr, "mm_prop_grad_backward: NULL proj");
     cudaStream_t st = (cudaStream_t)stream;
+    if (h->general)
+        return run_general<0, 3>(h, gu, gp, ntheta, j, true, st, proj, nullptr, inv_norm, inv_beta_ratio);
     MM_TRY((dispatch_y<0>(h, gu, ntheta, j, true, 0.f, 0.f, st)));
     return dispatch_x<3>(h, gp, ntheta, j, true, st, proj, nullptr, inv_norm, inv_beta_ratio);
 }

@@ -88,3 +88,25 @@ def test_autograd_function(case):
     (2.0 * loss).backward()
     _, g = m.loss_and_grad(dl.detach(), d32)
     assert torch.allclose(dl.grad, 2.0 * g, rtol=1e-6, atol=0)
+
+
+def test_general_sizes_gradient():
+    # n = 48, nz = 24: the Radon pair on its cuFFT path and D on the general
+    # (non-power-of-two) path, fused gradient against the FP64 oracle
+    from model_mosaic_b200.model import ForwardModel
+    from model_mosaic_b200.phantom import ellipsoid_volume
+    n, nz, T = 48, 24, 30
+    theta = np.linspace(0, np.pi, T, endpoint=False).astype(np.float32)
+    delta = ellipsoid_volume(n, nz, seed=0, vmin=0.2, vmax=1.0)
+    delta2 = ellipsoid_volume(n, nz, seed=1, vmin=0.2, vmax=1.0)
+    s = float(np.float32(1.5 / np.abs(ModelOracle(n, nz, theta, WL, VOX, DIST, s=1.0).tomo.R(delta)).max()))
+    ora = ModelOracle(n, nz, theta, WL, VOX, DIST, s=s)
+    d = ora.forward(delta2)
+    m = ForwardModel(n, nz, theta, WL, VOX, DIST, inv_norm=s, angle_chunk=16)
+    dl = torch.from_numpy(delta).cuda()
+    d32 = torch.from_numpy(d.astype(np.float32)).cuda()
+    loss, g = m.loss_and_grad(dl, d32)
+    assert abs(float(loss) - ora.loss(delta, d)) / ora.loss(delta, d) < 1e-5
+    assert rl2(g.cpu().numpy(), ora.grad(delta, d)) < 1e-5
+    l2, g2 = m.plain_loss_and_grad(dl, d32)
+    assert rl2(g.cpu().numpy(), g2.cpu().numpy()) < 1e-6
