@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rr2c(const TIN* _
 // R stage 5: Gaussian gather of the n/2+1 non-redundant samples per angle.
 // One group of LPS lanes per sample; each lane owns ZV slices.
 template <int ZV, int LPS, int M>
-__global__ void __launch_bounds__(kThreads, 4) k_gather(const float2* __restrict__ F, float2* __restrict__ H,
+__global__ void __launch_bounds__(kThreads, 3) k_gather(const float2* __restrict__ F, float2* __restrict__ H,
                                                      const float* __restrict__ cosT, const float* __restrict__ sinT,
                                                      int n, int T, int zs, float c0, float c1, float scale,
                                                      int clamp) {
@@ -476,7 +476,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_gather(const float2* __restrict
     const long zg = warp % zgroups;
     const long s = (warp / zgroups) * SPW + sub;
     if (s >= (long)T * K) return;
-    const int t = (int)(s / K), k = (int)(s % K);
+    // angle-major: consecutive warps take the same radius on consecutive
+    // angles, whose windows overlap most (and whose H rows are adjacent)
+    const int t = (int)(s % T), k = (int)(s / T);
     const SampleGeo g = sample_geo(t, k, n, M, cosT, sinT, clamp != 0);
     const float inv_twon = 1.0f / (float)(2 * n);
     float wx[L], wy[L];
