@@ -32,6 +32,7 @@ using mm::dev_alloc;
 
 struct mm_tomo {
     int n = 0, nz = 0, ntheta = 0, m = 0, zs = 0, K = 0, clamp = 0, compensated = 0;
+    int paired = 0;  // angles symmetric under theta -> theta + pi: the gather takes them in pairs
     float mu = 0.f, c0 = 0.f, c1 = 0.f, phi_scale = 0.f;
     int device = 0;
     float* d_cos = nullptr;
@@ -270,7 +271,7 @@ __global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xfwd(const TIN* _
     constexpr int n = L / 2, LP = L + L / 16, G = stockham::Sched<L>::G;
     extern __shared__ float2 sm[];
     const int g = threadIdx.x, l = threadIdx.y;
-    const int y = blockIdx.x, z0 = blockIdx.y * 4;
+    const int y = blockIdx.y, z0 = blockIdx.x * 4;  // z-groups fastest: a (v, u) segment fills at once
     const int za = z0 + 2 * l, zb = za + 1;
     const stockham::RowAddr ad{l * LP};
     const float py = phis * __ldg(phi1 + y);
@@ -322,7 +323,7 @@ __global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xinv(const float2
     constexpr int n = L / 2, LP = L + L / 16, G = stockham::Sched<L>::G;
     extern __shared__ float2 sm[];
     const int g = threadIdx.x, l = threadIdx.y;
-    const int y = blockIdx.x, z0 = blockIdx.y * 4;
+    const int y = blockIdx.y, z0 = blockIdx.x * 4;  // z-groups fastest: a (v, u) segment fills at once
     const int tid = l * G + g;
     const int nq = min(4, zs - z0);
     // one thread per u: load the four slices (one 32-byte sector), line h
@@ -459,6 +460,72 @@ __global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rr2c(const TIN* _
     }
 }
 
+// The 2m+1 taps of window row v (columns bx .. bx+2m), all loads issued
+// before any is used; taps outside the stored half plane are reflected and
+// conjugated (tap_cell).
+template <int ZV, int M>
+__device__ __forceinline__ void load_row(const float2* __restrict__ F, int bx, int v, bool fast, int n, int zs,
+                                         int zoff, float (&val)[2 * M + 1][2 * ZV]) {
+    constexpr int L = 2 * M + 1;
+    const long rowstride = (long)(n + 1) * zs;
+    const int twon = 2 * n;
+    if (fast) {
+        const int row = v < 0 ? v + twon : (v >= twon ? v - twon : v);
+        const float2* p = F + row * rowstride + (long)bx * zs + zoff;
+#pragma unroll
+        for (int i0 = 0; i0 < L; ++i0) ZVec<ZV>::load(p + (long)i0 * zs, val[i0]);
+    } else {
+#pragma unroll
+        for (int i0 = 0; i0 < L; ++i0) {
+            int row, col;
+            bool cj;
+            tap_cell(bx + i0, v, n, row, col, cj);
+            ZVec<ZV>::load(F + row * rowstride + (long)col * zs + zoff, val[i0]);
+            if (cj) {
+#pragma unroll
+                for (int q = 1; q < 2 * ZV; q += 2) val[i0][q] = -val[i0][q];
+            }
+        }
+    }
+}
+
+// Window sum of one sample: (2m+1)^2 taps, row partial sums along x first.
+template <int ZV, int M>
+__device__ __forceinline__ void window_sum(const float2* __restrict__ F, const SampleGeo& g, const float* wx,
+                                           const float* wy, float* acc, int n, int zs, int zoff) {
+    constexpr int L = 2 * M + 1;
+    const bool fast = (g.bx >= 0) && (g.bx + 2 * M <= n);
+#pragma unroll
+    for (int i1 = 0; i1 < L; ++i1) {
+        float val[L][2 * ZV];
+        load_row<ZV, M>(F, g.bx, g.by + i1, fast, n, zs, zoff, val);
+        float ar[2 * ZV];
+#pragma unroll
+        for (int q = 0; q < 2 * ZV; ++q) ar[q] = 0.f;
+#pragma unroll
+        for (int i0 = 0; i0 < L; ++i0) {
+#pragma unroll
+            for (int q = 0; q < 2 * ZV; ++q) ar[q] = fmaf(wx[i0], val[i0][q], ar[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < 2 * ZV; ++q) acc[q] = fmaf(wy[i1], ar[q], acc[q]);
+    }
+}
+
+// Sign of the C2R input slot and store of one gathered sample.
+template <int ZV>
+__device__ __forceinline__ void store_sample(float2* __restrict__ H, const SampleGeo& g, float* acc, int k, int t,
+                                             int n, int T, int zs, int zoff, float scale) {
+    const float sc = (g.j & 1) ? -scale : scale;
+    const float si = (k == 0 || k == n / 2) ? 0.f : (g.mir ? -sc : sc);
+#pragma unroll
+    for (int q = 0; q < 2 * ZV; q += 2) {
+        acc[q] *= sc;
+        acc[q + 1] *= si;
+    }
+    ZVec<ZV>::store(H + ((long)k * T + t) * zs + zoff, acc);
+}
+
 // R stage 5: Gaussian gather of the n/2+1 non-redundant samples per angle.
 // One group of LPS lanes per sample; each lane owns ZV slices.
 template <int ZV, int LPS, int M>
@@ -488,57 +555,83 @@ __global__ void __launch_bounds__(kThreads, 3) k_gather(const float2* __restrict
         wy[i] = c0 * tap_weight(g.by + i, g.y0, inv_twon, c1);
     }
     const int zoff = (int)zg * (LPS * ZV) + zl * ZV;
-    const long rowstride = (long)(n + 1) * zs;
-    const int twon = 2 * n;
     float acc[2 * ZV];
 #pragma unroll
     for (int q = 0; q < 2 * ZV; ++q) acc[q] = 0.f;
-    const bool fast = (g.bx >= 0) && (g.bx + 2 * M <= n);
-#pragma unroll
-    for (int i1 = 0; i1 < L; ++i1) {
-        float ar[2 * ZV];
-#pragma unroll
-        for (int q = 0; q < 2 * ZV; ++q) ar[q] = 0.f;
-        const int v = g.by + i1;
-        if (fast) {
-            const int row = v < 0 ? v + twon : (v >= twon ? v - twon : v);
-            const float2* p = F + row * rowstride + (long)g.bx * zs + zoff;
-#pragma unroll
-            for (int i0 = 0; i0 < L; ++i0) {
-                float val[2 * ZV];
-                ZVec<ZV>::load(p + (long)i0 * zs, val);
-#pragma unroll
-                for (int q = 0; q < 2 * ZV; ++q) ar[q] = fmaf(wx[i0], val[q], ar[q]);
-            }
-        } else {
-#pragma unroll
-            for (int i0 = 0; i0 < L; ++i0) {
-                int row, col;
-                bool cj;
-                tap_cell(g.bx + i0, v, n, row, col, cj);
-                float val[2 * ZV];
-                ZVec<ZV>::load(F + row * rowstride + (long)col * zs + zoff, val);
-                if (cj) {
-#pragma unroll
-                    for (int q = 1; q < 2 * ZV; q += 2) val[q] = -val[q];
-                }
-#pragma unroll
-                for (int q = 0; q < 2 * ZV; ++q) ar[q] = fmaf(wx[i0], val[q], ar[q]);
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 2 * ZV; ++q) acc[q] = fmaf(wy[i1], ar[q], acc[q]);
-    }
-    const float sc = (g.j & 1) ? -scale : scale;
+    window_sum<ZV, M>(F, g, wx, wy, acc, n, zs, zoff);
     // k = 0 and k = n/2 are the DC and Nyquist bins of the C2R along r: only
     // their real part enters the result (the .real of tomo.py:150)
-    const float si = (k == 0 || k == n / 2) ? 0.f : (g.mir ? -sc : sc);
+    store_sample<ZV>(H, g, acc, k, t, n, T, zs, zoff, scale);
+}
+
+// R stage 5 for angle sets symmetric under theta -> theta + pi (T even,
+// theta[t + T/2] = theta[t] + pi up to float32 rounding): the sample at radius
+// k of angle t + T/2 lies at the negated frequency of angle t's, which the
+// Hermitian fold maps back onto the same point, so the two usually share
+// their (2m+1)^2 window.  One lane group takes both samples; when the windows
+// coincide every tap is loaded once and weighted with each sample's own
+// weights, otherwise the two windows are summed one after the other.  Each
+// sample's arithmetic is exactly k_gather's (window_sum, store_sample).
+template <int ZV, int LPS, int M>
+__global__ void __launch_bounds__(kThreads, 2) k_gather_pair(const float2* __restrict__ F, float2* __restrict__ H,
+                                                          const float* __restrict__ cosT,
+                                                          const float* __restrict__ sinT, int n, int T, int zs,
+                                                          float c0, float c1, float scale, int clamp) {
+    constexpr int L = 2 * M + 1;
+    constexpr int SPW = 32 / LPS;
+    const int K = n / 2 + 1, T2 = T / 2;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / LPS, zl = lane % LPS;
+    const int zgroups = zs / (LPS * ZV);
+    const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long zg = warp % zgroups;
+    const long s = (warp / zgroups) * SPW + sub;
+    if (s >= (long)T2 * K) return;
+    const int t = (int)(s % T2), k = (int)(s / T2);
+    const SampleGeo ga = sample_geo(t, k, n, M, cosT, sinT, clamp != 0);
+    const SampleGeo gb = sample_geo(t + T2, k, n, M, cosT, sinT, clamp != 0);
+    const float inv_twon = 1.0f / (float)(2 * n);
+    float wxa[L], wya[L], wxb[L], wyb[L];
 #pragma unroll
-    for (int q = 0; q < 2 * ZV; q += 2) {
-        acc[q] *= sc;
-        acc[q + 1] *= si;
+    for (int i = 0; i < L; ++i) {
+        wxa[i] = tap_weight(ga.bx + i, ga.x0, inv_twon, c1);
+        wya[i] = c0 * tap_weight(ga.by + i, ga.y0, inv_twon, c1);
+        wxb[i] = tap_weight(gb.bx + i, gb.x0, inv_twon, c1);
+        wyb[i] = c0 * tap_weight(gb.by + i, gb.y0, inv_twon, c1);
     }
-    ZVec<ZV>::store(H + ((long)k * T + t) * zs + zoff, acc);
+    const int zoff = (int)zg * (LPS * ZV) + zl * ZV;
+    float acca[2 * ZV], accb[2 * ZV];
+#pragma unroll
+    for (int q = 0; q < 2 * ZV; ++q) acca[q] = accb[q] = 0.f;
+    if (ga.bx == gb.bx && ga.by == gb.by) {
+        const bool fast = (ga.bx >= 0) && (ga.bx + 2 * M <= n);
+#pragma unroll
+        for (int i1 = 0; i1 < L; ++i1) {
+            float val[L][2 * ZV];
+            load_row<ZV, M>(F, ga.bx, ga.by + i1, fast, n, zs, zoff, val);
+            float ara[2 * ZV], arb[2 * ZV];
+#pragma unroll
+            for (int q = 0; q < 2 * ZV; ++q) ara[q] = arb[q] = 0.f;
+#pragma unroll
+            for (int i0 = 0; i0 < L; ++i0) {
+#pragma unroll
+                for (int q = 0; q < 2 * ZV; ++q) {
+                    ara[q] = fmaf(wxa[i0], val[i0][q], ara[q]);
+                    arb[q] = fmaf(wxb[i0], val[i0][q], arb[q]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 2 * ZV; ++q) {
+                acca[q] = fmaf(wya[i1], ara[q], acca[q]);
+                accb[q] = fmaf(wyb[i1], arb[q], accb[q]);
+            }
+        }
+    } else {
+        window_sum<ZV, M>(F, ga, wxa, wya, acca, n, zs, zoff);
+        window_sum<ZV, M>(F, gb, wxb, wyb, accb, n, zs, zoff);
+    }
+    store_sample<ZV>(H, ga, acca, k, t, n, T, zs, zoff, scale);
+    store_sample<ZV>(H, gb, accb, k, t + T2, n, T, zs, zoff, scale);
 }
 
 // One term w*v of a scatter sum; KAHAN keeps a running compensation c of the
@@ -870,7 +963,7 @@ int launch_xfwd_l(mm_tomo* h, const void* obj, int nzc, cudaStream_t st) {
     const size_t smem = (size_t)2 * (L + L / 16) * sizeof(float2);
     auto kern = k_xfwd<L, TIN>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 block(G, 2), grid(h->n, (h->zs + 3) / 4);
+    dim3 block(G, 2), grid((h->zs + 3) / 4, h->n);
     kern<<<grid, block, smem, st>>>((const TIN*)obj, h->Y, h->d_phi1, h->phi_scale, h->d_twy, nzc, h->zs);
     MM_LAUNCHED();
     return MM_OK;
@@ -882,7 +975,7 @@ int launch_xinv_l(mm_tomo* h, void* obj, int nzc, cudaStream_t st) {
     const size_t smem = (size_t)2 * (L + L / 16) * sizeof(float2);
     auto kern = k_xinv<L, OUT, TOUT>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 block(G, 2), grid(h->n, (h->zs + 3) / 4);
+    dim3 block(G, 2), grid((h->zs + 3) / 4, h->n);
     kern<<<grid, block, smem, st>>>(h->Y, obj, h->d_phi1, h->phi_scale, h->d_twy, nzc, h->zs);
     MM_LAUNCHED();
     return MM_OK;
@@ -974,15 +1067,20 @@ int pick_lanes(int zs, int& ZV, int& LPS) {
 template <int ZV, int LPS>
 int launch_gather_m(mm_tomo* h, cudaStream_t st) {
     const int K = h->K;
-    const long samples = (long)h->ntheta * K;
+    const long samples = (long)(h->paired ? h->ntheta / 2 : h->ntheta) * K;  // paired: one lane group per pair
     const long warps = ((samples + (32 / LPS) - 1) / (32 / LPS)) * (h->zs / (LPS * ZV));
     const long blocks = (warps * 32 + kThreads - 1) / kThreads;
     const float scale = (float)(1.0 / (4.0 * h->n * (double)h->n));
-#define MM_G(MM)                                                                                 \
-    case MM:                                                                                     \
-        k_gather<ZV, LPS, MM><<<blocks, kThreads, 0, st>>>(h->F, h->Hh, h->d_cos, h->d_sin, h->n, \
-                                                           h->ntheta, h->zs, h->c0, h->c1, scale, \
-                                                           h->clamp);                              \
+#define MM_G(MM)                                                                                          \
+    case MM:                                                                                              \
+        if (h->paired)                                                                                    \
+            k_gather_pair<ZV, LPS, MM><<<blocks, kThreads, 0, st>>>(h->F, h->Hh, h->d_cos, h->d_sin, h->n, \
+                                                                    h->ntheta, h->zs, h->c0, h->c1, scale, \
+                                                                    h->clamp);                              \
+        else                                                                                              \
+            k_gather<ZV, LPS, MM><<<blocks, kThreads, 0, st>>>(h->F, h->Hh, h->d_cos, h->d_sin, h->n,      \
+                                                               h->ntheta, h->zs, h->c0, h->c1, scale,      \
+                                                               h->clamp);                                  \
         break;
     switch (h->m) {
         MM_G(2) MM_G(3) MM_G(4) MM_G(5) MM_G(6)
@@ -1157,6 +1255,14 @@ extern "C" int mm_tomo_create(int n, int nz, int ntheta, const float* theta_host
     };
     int rc;
     std::vector<float> cs(ntheta), sn(ntheta), ph(n);
+    if (ntheta % 2 == 0) {
+        bool sym = true;
+        for (int t = 0; t < ntheta / 2 && sym; ++t) {
+            const double d = fmod((double)theta_host[t + ntheta / 2] - (double)theta_host[t] + 4.0 * M_PI, 2.0 * M_PI);
+            sym = fabs(d - M_PI) < 1e-4;
+        }
+        h->paired = sym ? 1 : 0;
+    }
     for (int t = 0; t < ntheta; ++t) {
         cs[t] = (float)cos((double)theta_host[t]);
         sn[t] = (float)sin((double)theta_host[t]);

@@ -173,3 +173,20 @@ def test_production_size_n2048(TomoReal):
     ref = o64.RT(y[:, pick])
     floor = rl2(o32.RT(y[:, pick]), ref)
     assert rl2(tomo.RT(torch.from_numpy(y).cuda()).cpu().numpy()[pick], ref) < 1.5 * floor
+
+
+@pytest.mark.parametrize("n,nz", [(128, 64), (128, 16), (48, 8)])
+def test_paired_gather_360(TomoReal, n, nz):
+    # [0, 2 pi) with T even: angle t + T/2 = angle t + pi, so the gather takes
+    # the two in one lane group, sharing taps where their windows coincide.
+    # The same angles interleaved (no pairing) must give the same bits.
+    T = 90
+    theta = np.linspace(0, 2 * np.pi, T, endpoint=False).astype(np.float32)
+    perm = np.stack([np.arange(T // 2), np.arange(T // 2) + T // 2], axis=1).ravel()
+    rng = np.random.default_rng(n + nz)
+    x = rng.standard_normal((nz, n, n)).astype(np.float32)
+    xd = torch.from_numpy(x).cuda()
+    paired = TomoReal(n, nz, theta).R(xd)
+    single = TomoReal(n, nz, theta[perm]).R(xd)
+    assert torch.equal(paired[perm], single)
+    assert rl2(paired.cpu().numpy(), TomoRealOracle(n, nz, theta).R(x)) < RTOL
