@@ -231,11 +231,15 @@ __global__ void k_transpose_out(const float2* __restrict__ B, float2* __restrict
 // access is one 32-byte sector.  Forward: rows outside [n/2, 3n/2) are the
 // zero padding and are not read.  Inverse: only rows [n/2, 3n/2) are stored
 // (the x-C2R needs nothing else).  src/dst row stride = (n+1)*zs.
+// Forward: the gather reads only cells within radius n + m + 2 of the
+// spectrum origin (polar samples have |p| <= n cells, windows reach m + 1
+// further, reflected taps included), so rows outside radius n + 16 of each
+// column are not stored (about a fifth of the half plane).
 template <int L, bool INV>
 __global__ void __launch_bounds__(4 * stockham::Sched<L>::G) k_col_fft(const float2* __restrict__ src,
                                                                            float2* __restrict__ dst,
                                                                            const float2* __restrict__ tw,
-                                                                           long ncols) {
+                                                                           long ncols, int zs) {
     namespace sk = stockham;
     constexpr int CW = 4;
     extern __shared__ float2 sm[];
@@ -248,8 +252,14 @@ __global__ void __launch_bounds__(4 * stockham::Sched<L>::G) k_col_fft(const flo
         if (!INV && (pos < n / 2 || pos >= 3 * n / 2)) return make_float2(0.f, 0.f);
         return live ? __ldg(src + (long)pos * ncols + col) : make_float2(0.f, 0.f);
     };
+    const long u = col / zs;
+    const long r2max = (long)(n + 16) * (n + 16) - u * u;
     auto st = [&](int pos, float2 v) {
         if (INV && (pos < n / 2 || pos >= 3 * n / 2)) return;
+        if (!INV) {
+            const long vw = pos < n ? pos : pos - L;
+            if (vw * vw > r2max) return;
+        }
         if (live) dst[(long)pos * ncols + col] = v;
     };
     sk::fft<L, INV>(sm, ad, ld, st, g, tw);
@@ -935,7 +945,7 @@ int launch_col_fft_l(mm_tomo* h, const float2* src, float2* dst, cudaStream_t st
     auto kern = k_col_fft<L, INV>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 block(CW, G), grid((unsigned)((ncols + CW - 1) / CW));
-    kern<<<grid, block, smem, st>>>(src, dst, h->d_twy, ncols);
+    kern<<<grid, block, smem, st>>>(src, dst, h->d_twy, ncols, h->zs);
     MM_LAUNCHED();
     return MM_OK;
 }
