@@ -234,7 +234,9 @@ __global__ void k_transpose_out(const float2* __restrict__ B, float2* __restrict
 // Forward: the gather reads only cells within radius n + m + 2 of the
 // spectrum origin (polar samples have |p| <= n cells, windows reach m + 1
 // further, reflected taps included), so rows outside radius n + 16 of each
-// column are not stored (about a fifth of the half plane).
+// column are not stored (about a fifth of the half plane).  Inverse: the
+// scatter leaves those cells unwritten (they receive nothing), so they are
+// read as zeros.
 template <int L, bool INV>
 __global__ void __launch_bounds__(4 * stockham::Sched<L>::G) k_col_fft(const float2* __restrict__ src,
                                                                            float2* __restrict__ dst,
@@ -248,16 +250,20 @@ __global__ void __launch_bounds__(4 * stockham::Sched<L>::G) k_col_fft(const flo
     const bool live = col < ncols;
     const int n = L / 2;
     const sk::ColAddr<CW> ad{c};
+    const int u = (int)col / zs;
+    const int r2max = (n + 16) * (n + 16) - u * u;
     auto ld = [&](int pos) -> float2 {
         if (!INV && (pos < n / 2 || pos >= 3 * n / 2)) return make_float2(0.f, 0.f);
+        if (INV) {
+            const int vw = pos < n ? pos : pos - L;
+            if (vw * vw > r2max) return make_float2(0.f, 0.f);
+        }
         return live ? __ldg(src + (long)pos * ncols + col) : make_float2(0.f, 0.f);
     };
-    const long u = col / zs;
-    const long r2max = (long)(n + 16) * (n + 16) - u * u;
     auto st = [&](int pos, float2 v) {
         if (INV && (pos < n / 2 || pos >= 3 * n / 2)) return;
         if (!INV) {
-            const long vw = pos < n ? pos : pos - L;
+            const int vw = pos < n ? pos : pos - L;
             if (vw * vw > r2max) return;
         }
         if (live) dst[(long)pos * ncols + col] = v;
@@ -664,7 +670,7 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict
                                                       const unsigned* __restrict__ idx,
                                                       const float* __restrict__ wgt,
                                                       const float2* __restrict__ Q, float2* __restrict__ A,
-                                                      long ncells, int zs) {
+                                                      long ncells, int zs, int n, int prune) {
     constexpr int SPW = 32 / LPS;
     const int lane = threadIdx.x & 31;
     const int sub = lane / LPS, zl = lane % LPS;
@@ -673,6 +679,11 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict
     const long zg = warp % zgroups;
     const long c = (warp / zgroups) * SPW + sub;
     if (c >= ncells) return;
+    if (prune) {  // cells beyond radius n + 16 receive nothing; k_col_fft reads them as zeros
+        const int ci = (int)c, v = ci / (n + 1), u = ci - v * (n + 1);
+        const int vw = v < n ? v : v - 2 * n;
+        if (u * u + vw * vw > (n + 16) * (n + 16)) return;
+    }
     const int zoff = (int)zg * (LPS * ZV) + zl * ZV;
     float acc[2 * ZV], cmp[2 * ZV];
 #pragma unroll
@@ -1121,7 +1132,11 @@ int launch_scatter_t(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) {
     const long warps = ((ncells + (32 / LPS) - 1) / (32 / LPS)) * (h->zs / (LPS * ZV));
     const long blocks = (warps * 32 + kThreads - 1) / kThreads;
     auto kern = h->compensated ? k_scatter<ZV, LPS, true> : k_scatter<ZV, LPS, false>;
-    kern<<<blocks, kThreads, 0, st>>>(h->csr_ptr, h->csr_idx, h->csr_w, Q, A, ncells, h->zs);
+    // the native inverse column transform treats cells beyond radius n + 16
+    // as zeros; cuFFT (other sizes) reads them, so they are written then
+    const int L = 2 * h->n;
+    const int prune = (mm_is_pow2(L) && L >= 16 && L <= 4096) ? 1 : 0;
+    kern<<<blocks, kThreads, 0, st>>>(h->csr_ptr, h->csr_idx, h->csr_w, Q, A, ncells, h->zs, h->n, prune);
     MM_LAUNCHED();
     return MM_OK;
 }
