@@ -334,6 +334,79 @@ def run_model(args, local_rank):
     return out
 
 
+# ---------------------------------------------------------------- precision report
+def run_precision(args, local_rank):
+    """Relative L2 error against the FP64 oracle, per precision variant: float32
+    storage and arithmetic; bfloat16 storage of volume and sinogram with float32
+    arithmetic; Kahan-compensated adjoint scatter.  R and RT on a 64-slice slab
+    of the 1024^3 seeded volume at 1536 angles on [0, pi) (oracle on 2 of its
+    slices), D on 8 of the slab's frames, the model gradient on 128^3 with 192
+    angles (the FP64 oracle of the full 1024^3 model does not fit a host run)."""
+    import torch
+    from model_mosaic_b200.model import ForwardModel
+    from model_mosaic_b200.phantom import ellipsoid_volume, ellipsoid_volume_torch
+    from model_mosaic_b200.processing.propagation import Propagation
+    from model_mosaic_b200.processing.tomo import TomoReal
+    from oracle.fresnel import PropagationOracle, psi_from_proj
+    from oracle.model import ModelOracle
+    from oracle.usfft import TomoRealOracle
+
+    def rl2(a, b):
+        a = np.asarray(a, dtype=np.complex128 if np.iscomplexobj(a) else np.float64)
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    dev = torch.device("cuda", local_rank)
+    w = WORKLOADS["production"]
+    wl = 1.24e-9 / w["energy_kev"]
+    n, T, z0, nzs = 1024, 1536, 480, 64
+    theta = np.linspace(0, np.pi, T, endpoint=False).astype(np.float32)
+    pick = [0, 42]
+    x = ellipsoid_volume_torch(n, 1024, seed=0, device=dev)[z0:z0 + nzs].contiguous()
+    tomo = TomoReal(n, nzs, theta)
+    tomo_k = TomoReal(n, nzs, theta, compensated=True)
+    ora = TomoRealOracle(n, len(pick), theta)
+    xh = x[pick].cpu().numpy()
+    ref_r = ora.R(xh)
+    r32 = tomo.R(x)
+    rbf = tomo.R(x.to(torch.bfloat16))
+    rep = {"R": {"float32": rl2(r32[:, pick].cpu().numpy(), ref_r),
+                 "bfloat16_storage": rl2(rbf[:, pick].float().cpu().numpy(), ref_r)}}
+    y = r32
+    ref_rt = ora.RT(y[:, pick].cpu().numpy())
+    rep["RT"] = {"float32": rl2(tomo.RT(y)[pick].cpu().numpy(), ref_rt),
+                 "bfloat16_storage": rl2(tomo.RT(y.to(torch.bfloat16))[pick].float().cpu().numpy(), ref_rt),
+                 "kahan_scatter": rl2(tomo_k.RT(y)[pick].cpu().numpy(), ref_rt)}
+    s, ib = float(np.float32(1.0 / np.sqrt(n / T))), 0.01
+    p = (r32[:8] * (1.5 / float(r32.abs().max()))).cpu().numpy()          # phases up to 1.5 rad
+    psi = psi_from_proj(p, s, ib)
+    prop = Propagation(n, nzs, 8, 1, wl, w["voxelsize"], [w["distance"]])
+    ref_d = PropagationOracle(n, nzs, 8, 1, wl, w["voxelsize"], [w["distance"]]).D(psi, 0)
+    rep["D"] = {"float32": rl2(prop.D(torch.from_numpy(psi.astype(np.complex64)).to(dev), 0).cpu().numpy(), ref_d)}
+    ng, tg = 128, 192
+    thg = np.linspace(0, np.pi, tg, endpoint=False).astype(np.float32)
+    dg = ellipsoid_volume(ng, ng, seed=0, vmin=0.2, vmax=1.0)
+    dg2 = ellipsoid_volume(ng, ng, seed=1, vmin=0.2, vmax=1.0)
+    sg = float(np.float32(1.5 / np.abs(ModelOracle(ng, ng, thg, wl, w["voxelsize"], w["distance"], s=1.0)
+                                        .tomo.R(dg)).max()))
+    mo = ModelOracle(ng, ng, thg, wl, w["voxelsize"], w["distance"], s=sg)
+    data = mo.forward(dg2)
+    gref = mo.grad(dg, data)
+    rep["gradient"] = {}
+    for name, comp in (("float32", False), ("kahan_scatter", True)):
+        m = ForwardModel(ng, ng, thg, wl, w["voxelsize"], w["distance"], inv_norm=sg, angle_chunk=64,
+                         compensated=comp)
+        _, g = m.loss_and_grad(torch.from_numpy(dg).to(dev), torch.from_numpy(data.astype(np.float32)).to(dev))
+        rep["gradient"][name] = rl2(g.cpu().numpy(), gref)
+    rep = {k: {v: float(f"{e:.3e}") for v, e in d.items()} for k, d in rep.items()}
+    return {"precision_report": rep,
+            "config": {"R_RT": f"slices {z0}..{z0 + nzs - 1} of the seeded 1024^3 volume, {T} angles on [0, pi), "
+                               f"oracle on slices {[z0 + q for q in pick]}",
+                       "D": f"8 frames of {nzs}x{n} from those projections (phase scaled to 1.5 rad)",
+                       "gradient": f"{ng}^3, {tg} angles, FP64 oracle",
+                       "bfloat16_storage": "inputs and outputs stored as bfloat16, float32 arithmetic; "
+                                           "D and the gradient kernels take float32 only"}}
+
+
 # ---------------------------------------------------------------- CPU (reference kernels on the host)
 def cpu_sample(w, slices=1, frames=32, cores=None):
     """Time the reference's kernels + restated glue on a bounded sample and
@@ -400,6 +473,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-rt", action="store_true", help="skip the adjoint (no scatter table)")
     ap.add_argument("--no-model", action="store_true", help="skip the fwd+grad timing of the model")
+    ap.add_argument("--precision", action="store_true",
+                    help="print the precision report (errors vs the FP64 oracle per variant) instead of timing")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -411,6 +486,10 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args, w)), flush=True)
+        return
+    if args.precision:
+        if rank == 0:
+            print(json.dumps(run_precision(args, local_rank)), flush=True)
         return
 
     if world > 1:

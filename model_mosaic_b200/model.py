@@ -35,7 +35,7 @@ from model_mosaic_b200.processing.propagation import Propagation
 
 class ForwardModel:
     def __init__(self, n, nz, theta, wavelength, voxelsize, distance, *, inv_norm=None, beta_ratio=100.0,
-                 angle_chunk=None):
+                 angle_chunk=None, compensated=False):
         require_cuda()
         self.n, self.nz = int(n), int(nz)
         self.theta = np.asarray(theta).astype(np.float32)
@@ -43,7 +43,7 @@ class ForwardModel:
         self.s = float(np.float32(1.0 / np.sqrt(self.n / self.ntheta))) if inv_norm is None else float(inv_norm)
         self.ib = float(np.float32(1.0 / beta_ratio))
         self.chunk = int(angle_chunk or self.ntheta)
-        self.tomo = TomoReal(self.n, self.nz, self.theta)
+        self.tomo = TomoReal(self.n, self.nz, self.theta, compensated=compensated)
         self.prop = Propagation(self.n, self.nz, self.chunk, 1, wavelength, voxelsize, [float(distance)])
         self._gu = None
         self._partials = None
