@@ -921,6 +921,7 @@ int plan1d(cufftHandle* plan, long long len, long long istride, long long idist,
 // sequence on one stream); grown when a new plan needs more, and attached to
 // every plan each time a plan is added.
 int ensure_work(mm_tomo* h, size_t need) {
+    if (need == 0 && !h->fft_work) return MM_OK;  // no cuFFT plan needs scratch
     if (need > h->fft_work_bytes || !h->fft_work) {
         if (h->fft_work) {
             cudaFree(h->fft_work);
@@ -1221,8 +1222,10 @@ int ensure_rt(mm_tomo* h, cudaStream_t st) {
     if (!h->plans_rt) {
         const int n = h->n, T = h->ntheta, zs = h->zs;
         size_t ws = h->fft_work_bytes;
-        MM_TRY(plan1d(&h->plan_rr2c, n, 1, n, (long long)T * zs, 1, CUFFT_R2C, (long long)T * zs, &ws));
-        MM_TRY(plan1d(&h->plan_xc2r, 2 * n, 1, n + 1, 1, 2 * n, CUFFT_C2R, (long long)zs * n, &ws));
+        if (!h->fused_r)
+            MM_TRY(plan1d(&h->plan_rr2c, n, 1, n, (long long)T * zs, 1, CUFFT_R2C, (long long)T * zs, &ws));
+        if (!h->fused_x)
+            MM_TRY(plan1d(&h->plan_xc2r, 2 * n, 1, n + 1, 1, 2 * n, CUFFT_C2R, (long long)zs * n, &ws));
         h->plans_rt = true;
         MM_TRY(ensure_work(h, ws));
     }
@@ -1340,20 +1343,25 @@ extern "C" int mm_tomo_create(int n, int nz, int ntheta, const float* theta_host
         return fail(MM_ECUDA);
     }
     const size_t spec = (size_t)2 * n * (n + 1) * zs;
-    if ((rc = alloc(h, &h->P, (size_t)zs * n * 2 * n, "padded rows")) ||
-        (rc = alloc(h, &h->X, (size_t)zs * n * (n + 1), "row spectra")) ||
-        (rc = alloc(h, &h->Y, spec, "padded column input")) || (rc = alloc(h, &h->F, spec, "half spectrum")) ||
+    // P and X serve only the cuFFT x-side (sizes without the fused kernels)
+    if (!h->fused_x && ((rc = alloc(h, &h->P, (size_t)zs * n * 2 * n, "padded rows")) ||
+                        (rc = alloc(h, &h->X, (size_t)zs * n * (n + 1), "row spectra"))))
+        return fail(rc);
+    if ((rc = alloc(h, &h->Y, spec, "padded column input")) || (rc = alloc(h, &h->F, spec, "half spectrum")) ||
         (rc = alloc(h, &h->Hh, (size_t)h->K * ntheta * zs, "polar lines")))
         return fail(rc);
     if (cudaMemset(h->Y, 0, spec * sizeof(float2)) != cudaSuccess) {
         mm::set_error("mm_tomo_create: memset failed");
         return fail(MM_ECUDA);
     }
+    // cuFFT plans only where no native kernel covers the size
     size_t ws = 0;
-    if ((rc = plan1d(&h->plan_xr2c, 2 * n, 1, 2 * n, 1, n + 1, CUFFT_R2C, (long long)zs * n, &ws)) ||
-        (rc = plan1d(&h->plan_y, 2 * n, (long long)(n + 1) * zs, 1, (long long)(n + 1) * zs, 1, CUFFT_C2C,
-                     (long long)(n + 1) * zs, &ws)) ||
-        (rc = plan1d(&h->plan_rc2r, n, (long long)ntheta * zs, 1, 1, n, CUFFT_C2R, (long long)ntheta * zs, &ws)) ||
+    const bool native_col = mm_is_pow2(2L * n) && 2 * n >= 16 && 2 * n <= 4096;
+    if ((!h->fused_x && (rc = plan1d(&h->plan_xr2c, 2 * n, 1, 2 * n, 1, n + 1, CUFFT_R2C, (long long)zs * n, &ws))) ||
+        (!native_col && (rc = plan1d(&h->plan_y, 2 * n, (long long)(n + 1) * zs, 1, (long long)(n + 1) * zs, 1,
+                                     CUFFT_C2C, (long long)(n + 1) * zs, &ws))) ||
+        (!h->fused_r &&
+         (rc = plan1d(&h->plan_rc2r, n, (long long)ntheta * zs, 1, 1, n, CUFFT_C2R, (long long)ntheta * zs, &ws))) ||
         (rc = ensure_work(h, ws)))
         return fail(rc);
     if (cudaDeviceSynchronize() != cudaSuccess) {
