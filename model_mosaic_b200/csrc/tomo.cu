@@ -1082,7 +1082,8 @@ int launch_r(mm_tomo* h, bool inv, const void* src, void* dst, cudaStream_t st, 
 
 int pick_lanes(int zs, int& ZV, int& LPS) {
     if (zs >= 64) { ZV = 2; LPS = 32; }
-    else { ZV = 1; LPS = zs; }
+    else if (zs >= 2) { ZV = 2; LPS = zs / 2; }
+    else { ZV = 1; LPS = 1; }
     return MM_OK;
 }
 
@@ -1116,14 +1117,14 @@ int launch_gather_m(mm_tomo* h, cudaStream_t st) {
 int launch_gather(mm_tomo* h, cudaStream_t st) {
     int ZV, LPS;
     pick_lanes(h->zs, ZV, LPS);
-    if (ZV == 2) return launch_gather_m<2, 32>(h, st);
+    if (ZV == 1) return launch_gather_m<1, 1>(h, st);
     switch (LPS) {
-        case 1: return launch_gather_m<1, 1>(h, st);
-        case 2: return launch_gather_m<1, 2>(h, st);
-        case 4: return launch_gather_m<1, 4>(h, st);
-        case 8: return launch_gather_m<1, 8>(h, st);
-        case 16: return launch_gather_m<1, 16>(h, st);
-        default: return launch_gather_m<1, 32>(h, st);
+        case 1: return launch_gather_m<2, 1>(h, st);
+        case 2: return launch_gather_m<2, 2>(h, st);
+        case 4: return launch_gather_m<2, 4>(h, st);
+        case 8: return launch_gather_m<2, 8>(h, st);
+        case 16: return launch_gather_m<2, 16>(h, st);
+        default: return launch_gather_m<2, 32>(h, st);
     }
 }
 
@@ -1145,14 +1146,14 @@ int launch_scatter_t(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) {
 int launch_scatter(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) {
     int ZV, LPS;
     pick_lanes(h->zs, ZV, LPS);
-    if (ZV == 2) return launch_scatter_t<2, 32>(h, Q, A, st);
+    if (ZV == 1) return launch_scatter_t<1, 1>(h, Q, A, st);
     switch (LPS) {
-        case 1: return launch_scatter_t<1, 1>(h, Q, A, st);
-        case 2: return launch_scatter_t<1, 2>(h, Q, A, st);
-        case 4: return launch_scatter_t<1, 4>(h, Q, A, st);
-        case 8: return launch_scatter_t<1, 8>(h, Q, A, st);
-        case 16: return launch_scatter_t<1, 16>(h, Q, A, st);
-        default: return launch_scatter_t<1, 32>(h, Q, A, st);
+        case 1: return launch_scatter_t<2, 1>(h, Q, A, st);
+        case 2: return launch_scatter_t<2, 2>(h, Q, A, st);
+        case 4: return launch_scatter_t<2, 4>(h, Q, A, st);
+        case 8: return launch_scatter_t<2, 8>(h, Q, A, st);
+        case 16: return launch_scatter_t<2, 16>(h, Q, A, st);
+        default: return launch_scatter_t<2, 32>(h, Q, A, st);
     }
 }
 
