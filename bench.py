@@ -85,27 +85,35 @@ def profile_traffic(workload, kernel):
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi sampling of SM clocks and throttle reasons.  The sampler runs
+    from before the warm-up to after the last timed loop (every 25 ms, with
+    timestamps); the summary keeps the samples that fall inside the timed
+    regions (``window`` marks each)."""
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.lines = []
+        self.windows = []
 
-    def __enter__(self):
+    def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "25"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
         return self
 
-    def __exit__(self, *a):
-        self.lines = []
+    def window(self, t0, t1):
+        self.windows.append((t0, t1))
+
+    def stop(self):
         if self.proc:
+            time.sleep(0.1)
             self.proc.terminate()
             try:
                 out, _ = self.proc.communicate(timeout=5)
@@ -113,26 +121,32 @@ class Clocks:
                 self.proc.kill()
                 out = ""
             self.lines = [l for l in out.splitlines() if l.strip()]
+            self.proc = None
 
     def summary(self):
+        import datetime
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in getattr(self, "lines", []):
+        for l in self.lines:
             f = [x.strip() for x in l.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                mx.append(float(f[2]))
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                smv, mxv = float(f[2]), float(f[3])
             except ValueError:
                 continue
-            for nm, v in zip(names, f[5:9]):
+            if not any(t0 - 0.03 <= ts <= t1 + 0.03 for t0, t1 in self.windows):
+                continue
+            sm.append(smv)
+            mx.append(mxv)
+            for nm, v in zip(names, f[6:10]):
                 if v.lower() == "active":
                     reasons.add(nm)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "sampled": "nvidia-smi every 25 ms inside the timed step, RT and e2e loops"}
 
 
 # ---------------------------------------------------------------- our arm
@@ -165,6 +179,8 @@ def run_ours(args, w, rank, world, local_rank):
         tomo.R_into(obj, sino)
         prop.intensity_into(sino, inten, inv_norm, inv_beta)
 
+    clk = Clocks(local_rank).start()   # running before the warm-up, stopped after the last timed loop
+
     def barrier():
         if world > 1:
             dist.barrier()
@@ -181,14 +197,15 @@ def run_ours(args, w, rank, world, local_rank):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
-    with Clocks(local_rank) as clk:
-        torch.cuda.nvtx.range_push("timed_step")
-        e0.record(st)
-        for _ in range(args.steps):
-            step()
-        e1.record(st)
-        torch.cuda.nvtx.range_pop()
-        torch.cuda.synchronize()
+    t_w0 = time.time()
+    torch.cuda.nvtx.range_push("timed_step")
+    e0.record(st)
+    for _ in range(args.steps):
+        step()
+    e1.record(st)
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    clk.window(t_w0, time.time())
     barrier()
     ms_step = max_over_ranks(e0.elapsed_time(e1) / args.steps)
     tstages, tk = tomo.timing()
@@ -204,6 +221,7 @@ def run_ours(args, w, rank, world, local_rank):
         tomo.set_timing(True)
         barrier()
         torch.cuda.synchronize()
+        t_w0 = time.time()
         torch.cuda.nvtx.range_push("timed_rt")
         e0.record(st)
         for _ in range(args.steps):
@@ -211,6 +229,7 @@ def run_ours(args, w, rank, world, local_rank):
         e1.record(st)
         torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
+        clk.window(t_w0, time.time())
         ms_rt = max_over_ranks(e0.elapsed_time(e1) / args.steps)
         rtstages, _ = tomo.timing()
         tomo.set_timing(False)
@@ -227,6 +246,7 @@ def run_ours(args, w, rank, world, local_rank):
         fwd.submit(obj_h, outs_h[i % 2])
     fwd.synchronize()
     barrier()
+    t_w0 = time.time()
     torch.cuda.nvtx.range_push("timed_e2e")
     e0.record(fwd.s_in)
     for i in range(args.steps):
@@ -234,6 +254,8 @@ def run_ours(args, w, rank, world, local_rank):
     e1.record(fwd.s_out)
     torch.cuda.nvtx.range_pop()
     fwd.synchronize()
+    clk.window(t_w0, time.time())
+    clk.stop()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1) / args.steps)
     fwd.free()
 
