@@ -22,6 +22,7 @@
 #include "fft_smem.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 #include <cuda_bf16.h>
 #include <math.h>
 
@@ -56,9 +57,9 @@ struct mm_tomo {
     bool y_dirty = false;        // RT used Y as scratch: its zero pad rows need restoring
     // adjoint scatter table
     bool csr_ready = false;
-    unsigned* csr_ptr = nullptr;  // ncells + 1
-    unsigned* csr_idx = nullptr;  // sample index (k*T + t) | conj << 31
-    float* csr_w = nullptr;
+    unsigned* csr_ptr = nullptr;  // npairs + 1 (cell pairs (row, 2p), (row, 2p+1))
+    unsigned* csr_idx = nullptr;  // sample index (k*T + t) | conj left << 31 | conj right << 30
+    float2* csr_w = nullptr;      // (left, right) weights
     size_t nnz = 0;
     float* ypad = nullptr;       // (T, zs, n) real sino padded in z (nz < zs)
     float2* yc = nullptr;        // (T, zs, n) complex sino spectrum (complex RT)
@@ -664,39 +665,58 @@ __device__ __forceinline__ void acc_add(float& s, float& c, float w, float v) {
     }
 }
 
-// RT: pull-scatter over the static CSR table.  One lane group per cell.
+// RT: pull-scatter over the static pair table.  One lane group per pair of
+// horizontally adjacent cells (row, 2p) and (row, 2p+1): the two cells
+// receive almost the same samples (8 of a window's 9 columns cover both), so
+// each table entry carries the sample's weight for either cell and the
+// sample's spectrum row is loaded once for both.  idx bit 31 / bit 30:
+// conjugate for the left / right cell.
 template <int ZV, int LPS, bool KAHAN>
 __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict__ ptr,
                                                       const unsigned* __restrict__ idx,
-                                                      const float* __restrict__ wgt,
+                                                      const float2* __restrict__ wgt,
                                                       const float2* __restrict__ Q, float2* __restrict__ A,
-                                                      long ncells, int zs, int n, int prune) {
+                                                      long npairs, int zs, int n, int prune) {
     constexpr int SPW = 32 / LPS;
     const int lane = threadIdx.x & 31;
     const int sub = lane / LPS, zl = lane % LPS;
     const int zgroups = zs / (LPS * ZV);
     const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long zg = warp % zgroups;
-    const long c = (warp / zgroups) * SPW + sub;
-    if (c >= ncells) return;
-    if (prune) {  // cells beyond radius n + 16 receive nothing; k_col_fft reads them as zeros
-        const int ci = (int)c, v = ci / (n + 1), u = ci - v * (n + 1);
-        const int vw = v < n ? v : v - 2 * n;
-        if (u * u + vw * vw > (n + 16) * (n + 16)) return;
-    }
+    const long p = (warp / zgroups) * SPW + sub;
+    if (p >= npairs) return;
+    const int NP = n / 2 + 1;
+    const int row = (int)(p / NP), c0 = (int)(p % NP) * 2;
+    // cells beyond radius n + 16 receive nothing; with `prune` they are not
+    // written (k_col_fft reads them as zeros)
+    const int vw = row < n ? row : row - 2 * n;
+    const int lim = (n + 16) * (n + 16) - vw * vw;
+    const bool keepL = !prune || c0 * c0 <= lim;
+    const bool keepR = c0 + 1 <= n && (!prune || (c0 + 1) * (c0 + 1) <= lim);
+    if (!keepL && !keepR) return;
     const int zoff = (int)zg * (LPS * ZV) + zl * ZV;
-    float acc[2 * ZV], cmp[2 * ZV];
+    float al[2 * ZV], cl[2 * ZV], ar[2 * ZV], cr[2 * ZV];
 #pragma unroll
-    for (int q = 0; q < 2 * ZV; ++q) acc[q] = cmp[q] = 0.f;
-    const unsigned e0 = __ldg(ptr + c), e1 = __ldg(ptr + c + 1);
+    for (int q = 0; q < 2 * ZV; ++q) al[q] = cl[q] = ar[q] = cr[q] = 0.f;
+    auto add = [&](unsigned ii, float2 w, const float* v) {
+        const float sl = (ii >> 31) ? -w.x : w.x, sr = ((ii >> 30) & 1u) ? -w.y : w.y;
+#pragma unroll
+        for (int q = 0; q < 2 * ZV; q += 2) {
+            acc_add<KAHAN>(al[q], cl[q], w.x, v[q]);
+            acc_add<KAHAN>(al[q + 1], cl[q + 1], sl, v[q + 1]);
+            acc_add<KAHAN>(ar[q], cr[q], w.y, v[q]);
+            acc_add<KAHAN>(ar[q + 1], cr[q + 1], sr, v[q + 1]);
+        }
+    };
+    const unsigned e0 = __ldg(ptr + p), e1 = __ldg(ptr + p + 1);
     if constexpr (LPS == 32) {
-        // one cell per warp: 32 table entries per coalesced load, handed out
-        // by shuffles, four independent value loads in flight
+        // one pair per warp: 32 table entries per coalesced load, handed out
+        // by shuffles, four independent spectrum loads in flight
         const unsigned FULL = 0xffffffffu;
         for (unsigned base = e0; base < e1; base += 32) {
             const int cnt = (int)min(32u, e1 - base);
             unsigned mi = 0;
-            float mw = 0.f;
+            float2 mw = make_float2(0.f, 0.f);
             if (lane < cnt) {
                 mi = __ldg(idx + base + lane);
                 mw = __ldg(wgt + base + lane);
@@ -704,129 +724,153 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict
             int k = 0;
             for (; k + 4 <= cnt; k += 4) {
                 unsigned ii[4];
-                float ww[4], vv[4][2 * ZV];
+                float2 ww[4];
+                float vv[4][2 * ZV];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     ii[u] = __shfl_sync(FULL, mi, k + u);
-                    ww[u] = __shfl_sync(FULL, mw, k + u);
+                    ww[u].x = __shfl_sync(FULL, mw.x, k + u);
+                    ww[u].y = __shfl_sync(FULL, mw.y, k + u);
                 }
 #pragma unroll
-                for (int u = 0; u < 4; ++u) ZVec<ZV>::load(Q + (long)(ii[u] & 0x7fffffffu) * zs + zoff, vv[u]);
+                for (int u = 0; u < 4; ++u) ZVec<ZV>::load(Q + (long)(ii[u] & 0x3fffffffu) * zs + zoff, vv[u]);
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const float sw = (ii[u] >> 31) ? -ww[u] : ww[u];
-#pragma unroll
-                    for (int q = 0; q < 2 * ZV; q += 2) {
-                        acc_add<KAHAN>(acc[q], cmp[q], ww[u], vv[u][q]);
-                        acc_add<KAHAN>(acc[q + 1], cmp[q + 1], sw, vv[u][q + 1]);
-                    }
-                }
+                for (int u = 0; u < 4; ++u) add(ii[u], ww[u], vv[u]);
             }
             for (; k < cnt; ++k) {
                 const unsigned ia = __shfl_sync(FULL, mi, k);
-                const float wa = __shfl_sync(FULL, mw, k);
+                float2 wa;
+                wa.x = __shfl_sync(FULL, mw.x, k);
+                wa.y = __shfl_sync(FULL, mw.y, k);
                 float va[2 * ZV];
-                ZVec<ZV>::load(Q + (long)(ia & 0x7fffffffu) * zs + zoff, va);
-                const float sa = (ia >> 31) ? -wa : wa;
-#pragma unroll
-                for (int q = 0; q < 2 * ZV; q += 2) {
-                    acc_add<KAHAN>(acc[q], cmp[q], wa, va[q]);
-                    acc_add<KAHAN>(acc[q + 1], cmp[q + 1], sa, va[q + 1]);
-                }
+                ZVec<ZV>::load(Q + (long)(ia & 0x3fffffffu) * zs + zoff, va);
+                add(ia, wa, va);
             }
         }
-        ZVec<ZV>::store(A + c * zs + zoff, acc);
-        return;
-    }
-    unsigned e = e0;
-    for (; e + 2 <= e1; e += 2) {
-        const unsigned ia = __ldg(idx + e), ib = __ldg(idx + e + 1);
-        const float wa = __ldg(wgt + e), wb = __ldg(wgt + e + 1);
-        float va[2 * ZV], vb[2 * ZV];
-        ZVec<ZV>::load(Q + (long)(ia & 0x7fffffffu) * zs + zoff, va);
-        ZVec<ZV>::load(Q + (long)(ib & 0x7fffffffu) * zs + zoff, vb);
-        const float sa = (ia >> 31) ? -wa : wa, sb = (ib >> 31) ? -wb : wb;
-#pragma unroll
-        for (int q = 0; q < 2 * ZV; q += 2) {
-            acc_add<KAHAN>(acc[q], cmp[q], wa, va[q]);
-            acc_add<KAHAN>(acc[q + 1], cmp[q + 1], sa, va[q + 1]);
+    } else {
+        unsigned e = e0;
+        for (; e + 2 <= e1; e += 2) {
+            const unsigned ia = __ldg(idx + e), ib = __ldg(idx + e + 1);
+            const float2 wa = __ldg(wgt + e), wb = __ldg(wgt + e + 1);
+            float va[2 * ZV], vb[2 * ZV];
+            ZVec<ZV>::load(Q + (long)(ia & 0x3fffffffu) * zs + zoff, va);
+            ZVec<ZV>::load(Q + (long)(ib & 0x3fffffffu) * zs + zoff, vb);
+            add(ia, wa, va);
+            add(ib, wb, vb);
         }
-#pragma unroll
-        for (int q = 0; q < 2 * ZV; q += 2) {
-            acc_add<KAHAN>(acc[q], cmp[q], wb, vb[q]);
-            acc_add<KAHAN>(acc[q + 1], cmp[q + 1], sb, vb[q + 1]);
+        if (e < e1) {
+            const unsigned ia = __ldg(idx + e);
+            const float2 wa = __ldg(wgt + e);
+            float va[2 * ZV];
+            ZVec<ZV>::load(Q + (long)(ia & 0x3fffffffu) * zs + zoff, va);
+            add(ia, wa, va);
         }
     }
-    if (e < e1) {
-        const unsigned ia = __ldg(idx + e);
-        const float wa = __ldg(wgt + e);
-        float va[2 * ZV];
-        ZVec<ZV>::load(Q + (long)(ia & 0x7fffffffu) * zs + zoff, va);
-        const float sa = (ia >> 31) ? -wa : wa;
-#pragma unroll
-        for (int q = 0; q < 2 * ZV; q += 2) {
-            acc_add<KAHAN>(acc[q], cmp[q], wa, va[q]);
-            acc_add<KAHAN>(acc[q + 1], cmp[q + 1], sa, va[q + 1]);
-        }
-    }
-    ZVec<ZV>::store(A + c * zs + zoff, acc);
+    const long cell = (long)row * (n + 1) + c0;
+    if (keepL) ZVec<ZV>::store(A + cell * zs + zoff, al);
+    if (keepR) ZVec<ZV>::store(A + (cell + 1) * zs + zoff, ar);
 }
 
 // Scatter-table construction ---------------------------------------------
-// Key of entry e = (sample s, tap): (cell << 32) | e, with e = s*L*L + tap.
+// Every tap e = (sample s, tap) of every polar sample gets the key
+//   (pair << 33) | (e << 1) | half,  pair = row * (n/2+1) + col/2, half = col & 1,
+// for its destination cell (row, col); sorted, the taps of one cell pair come
+// in sample order, and a left-cell tap followed by the same sample's
+// right-cell tap merges into one entry.
 template <int M>
-__global__ void k_csr_keys(unsigned long long* __restrict__ keys, const float* __restrict__ cosT,
-                           const float* __restrict__ sinT, int n, int T, long nent) {
+__device__ __forceinline__ void tap_dest(long e, int n, int T, const float* __restrict__ cosT,
+                                         const float* __restrict__ sinT, SampleGeo& g, int& k, int& t, int& i0,
+                                         int& i1, int& row, int& col, bool& cj) {
     constexpr int L = 2 * M + 1;
-    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nent) return;
     const int K = n / 2 + 1;
     const long s = e / (L * L);
     const int tap = (int)(e % (L * L));
-    const int t = (int)(s / K), k = (int)(s % K);
-    const SampleGeo g = sample_geo(t, k, n, M, cosT, sinT);
-    int row, col;
-    bool cj;
-    tap_cell(g.bx + tap % L, g.by + tap / L, n, row, col, cj);
-    const unsigned long long cell = (unsigned long long)row * (n + 1) + col;
-    keys[e] = (cell << 32) | (unsigned long long)e;
+    t = (int)(s / K);
+    k = (int)(s % K);
+    g = sample_geo(t, k, n, M, cosT, sinT);
+    i0 = tap % L;
+    i1 = tap / L;
+    tap_cell(g.bx + i0, g.by + i1, n, row, col, cj);
 }
 
 template <int M>
-__global__ void k_csr_payload(const unsigned long long* __restrict__ keys, unsigned* __restrict__ idx,
-                              float* __restrict__ wgt, const float* __restrict__ cosT,
-                              const float* __restrict__ sinT, int n, int T, long nent, float c0, float c1,
-                              float scale) {
-    constexpr int L = 2 * M + 1;
+__global__ void k_pair_keys(unsigned long long* __restrict__ keys, const float* __restrict__ cosT,
+                            const float* __restrict__ sinT, int n, int T, long nent) {
+    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nent) return;
+    SampleGeo g;
+    int k, t, i0, i1, row, col;
+    bool cj;
+    tap_dest<M>(e, n, T, cosT, sinT, g, k, t, i0, i1, row, col, cj);
+    const unsigned long long pair = (unsigned long long)row * (n / 2 + 1) + (col >> 1);
+    keys[e] = (pair << 33) | ((unsigned long long)e << 1) | (unsigned long long)(col & 1);
+}
+
+// head[i] = 0 when sorted tap i is the right half merged into tap i-1.
+template <int M>
+__global__ void k_pair_heads(const unsigned long long* __restrict__ keys, unsigned* __restrict__ head, long nent) {
+    constexpr int LL = (2 * M + 1) * (2 * M + 1);
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nent) return;
-    const long e = (long)(keys[i] & 0xffffffffull);
-    const int K = n / 2 + 1;
-    const long s = e / (L * L);
-    const int tap = (int)(e % (L * L));
-    const int t = (int)(s / K), k = (int)(s % K);
-    const SampleGeo g = sample_geo(t, k, n, M, cosT, sinT);
-    const int i0 = tap % L, i1 = tap / L;
+    unsigned h = 1;
+    if (i > 0) {
+        const unsigned long long a = keys[i - 1], b = keys[i];
+        const bool same_pair = (a >> 33) == (b >> 33);
+        const bool same_sample = ((a >> 1) & 0xffffffffull) / LL == ((b >> 1) & 0xffffffffull) / LL;
+        if (same_pair && same_sample && (a & 1) == 0 && (b & 1) == 1) h = 0;
+    }
+    head[i] = h;
+}
+
+template <int M>
+__device__ __forceinline__ float tap_wgt(const SampleGeo& g, int k, int i0, int i1, int n, float c0, float c1,
+                                         float scale) {
     const float inv_twon = 1.0f / (float)(2 * n);
     const float wx = tap_weight(g.bx + i0, g.x0, inv_twon, c1);
     const float wy = c0 * tap_weight(g.by + i1, g.y0, inv_twon, c1);
-    int row, col;
-    bool cj;
-    tap_cell(g.bx + i0, g.by + i1, n, row, col, cj);
     // transpose of H = (-1)^j g / (4n^2) followed by the C2R along r, which
     // counts the interior bins twice
     const float ck = (k > 0 && k < n / 2) ? 2.f : 1.f;
     const float sj = (g.j & 1) ? -1.f : 1.f;
-    wgt[i] = (wy * wx) * (ck * sj * scale);
-    idx[i] = (unsigned)((long)k * T + t) | ((cj != g.mir) ? 0x80000000u : 0u);
+    return (wy * wx) * (ck * sj * scale);
 }
 
-__global__ void k_csr_ptr(const unsigned long long* __restrict__ keys, unsigned* __restrict__ ptr, long nent,
-                          long ncells) {
+// Compacted entry of every head: sample index (k*T + t) with the two conj
+// bits, (left, right) weights, and its pair for the row pointers.
+template <int M>
+__global__ void k_pair_payload(const unsigned long long* __restrict__ keys, const unsigned* __restrict__ head,
+                               const unsigned* __restrict__ pos, unsigned* __restrict__ idx,
+                               float2* __restrict__ wgt, unsigned* __restrict__ pairs,
+                               const float* __restrict__ cosT, const float* __restrict__ sinT, int n, int T,
+                               long nent, float c0, float c1, float scale) {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i > nent) return;
-    const long prev = (i == 0) ? -1 : (long)(keys[i - 1] >> 32);
-    const long cur = (i == nent) ? ncells : (long)(keys[i] >> 32);
+    if (i >= nent || !head[i]) return;
+    const bool merged = i + 1 < nent && !head[i + 1];
+    float w[2] = {0.f, 0.f};
+    unsigned conj = 0, sidx = 0;
+    for (long j = i; j <= (merged ? i + 1 : i); ++j) {
+        const unsigned long long key = keys[j];
+        SampleGeo g;
+        int k, t, i0, i1, row, col;
+        bool cj;
+        tap_dest<M>((long)((key >> 1) & 0xffffffffull), n, T, cosT, sinT, g, k, t, i0, i1, row, col, cj);
+        const int half = (int)(key & 1);
+        w[half] = tap_wgt<M>(g, k, i0, i1, n, c0, c1, scale);
+        if (cj != g.mir) conj |= half ? 0x40000000u : 0x80000000u;
+        sidx = (unsigned)((long)k * T + t);
+    }
+    const unsigned o = pos[i];
+    idx[o] = sidx | conj;
+    wgt[o] = make_float2(w[0], w[1]);
+    pairs[o] = (unsigned)(keys[i] >> 33);
+}
+
+// ptr[p] = first entry of pair p (entries sorted by pair).
+__global__ void k_pair_ptr(const unsigned* __restrict__ pairs, unsigned* __restrict__ ptr, long nnz, long npairs) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > nnz) return;
+    const long prev = (i == 0) ? -1 : (long)pairs[i - 1];
+    const long cur = (i == nnz) ? npairs : (long)pairs[i];
     for (long c = prev + 1; c <= cur; ++c) ptr[c] = (unsigned)i;
 }
 
@@ -1130,15 +1174,15 @@ int launch_gather(mm_tomo* h, cudaStream_t st) {
 
 template <int ZV, int LPS>
 int launch_scatter_t(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) {
-    const long ncells = 2L * h->n * (h->n + 1);
-    const long warps = ((ncells + (32 / LPS) - 1) / (32 / LPS)) * (h->zs / (LPS * ZV));
+    const long npairs = 2L * h->n * (h->n / 2 + 1);
+    const long warps = ((npairs + (32 / LPS) - 1) / (32 / LPS)) * (h->zs / (LPS * ZV));
     const long blocks = (warps * 32 + kThreads - 1) / kThreads;
     auto kern = h->compensated ? k_scatter<ZV, LPS, true> : k_scatter<ZV, LPS, false>;
     // the native inverse column transform treats cells beyond radius n + 16
     // as zeros; cuFFT (other sizes) reads them, so they are written then
     const int L = 2 * h->n;
     const int prune = (mm_is_pow2(L) && L >= 16 && L <= 4096) ? 1 : 0;
-    kern<<<blocks, kThreads, 0, st>>>(h->csr_ptr, h->csr_idx, h->csr_w, Q, A, ncells, h->zs, h->n, prune);
+    kern<<<blocks, kThreads, 0, st>>>(h->csr_ptr, h->csr_idx, h->csr_w, Q, A, npairs, h->zs, h->n, prune);
     MM_LAUNCHED();
     return MM_OK;
 }
@@ -1162,31 +1206,39 @@ int build_csr(mm_tomo* h, cudaStream_t st) {
     h->tm.begin(12, st);
     const int n = h->n, T = h->ntheta, M = h->m, L = 2 * M + 1;
     const long nent = (long)T * h->K * L * L;
-    const long ncells = 2L * n * (n + 1);
-    MM_REQUIRE(nent < (1L << 32) && (long)T * h->K < (1L << 31), "adjoint table too large: %ld entries", nent);
-    int cellbits = 1;
-    while ((1L << cellbits) < ncells) ++cellbits;
+    const long npairs = 2L * n * (n / 2 + 1);
+    MM_REQUIRE(nent < (1L << 32) && (long)T * h->K < (1L << 30), "adjoint table too large: %ld entries", nent);
+    int pairbits = 1;
+    while ((1L << pairbits) < npairs) ++pairbits;
+    MM_REQUIRE(33 + pairbits <= 64, "adjoint table too large: %ld cell pairs", npairs);
     unsigned long long *kin = nullptr, *kout = nullptr;
+    unsigned *head = nullptr, *pos = nullptr, *pairs = nullptr;
     void* tmp = nullptr;
-    size_t tmp_bytes = 0;
+    size_t tmp_bytes = 0, scan_bytes = 0;
     int rc = MM_OK;
     auto cleanup = [&]() {
-        if (kin) cudaFree(kin);
-        if (kout) cudaFree(kout);
-        if (tmp) cudaFree(tmp);
+        void* bufs[] = {kin, kout, head, pos, pairs, tmp};
+        for (void* b : bufs)
+            if (b) cudaFree(b);
+    };
+    auto fail_cuda = [&](cudaError_t e) {
+        cleanup();
+        mm::set_error("building the adjoint scatter table: %s", cudaGetErrorString(e));
+        return MM_ECUDA;
     };
     if ((rc = dev_alloc((void**)&kin, nent * 8, "scatter keys")) != MM_OK) return cleanup(), rc;
     if ((rc = dev_alloc((void**)&kout, nent * 8, "scatter keys (sorted)")) != MM_OK) return cleanup(), rc;
-    cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, kin, kout, (int64_t)nent, 0, 32 + cellbits, st);
-    if ((rc = dev_alloc(&tmp, tmp_bytes, "radix sort temp")) != MM_OK) return cleanup(), rc;
-    if ((rc = alloc(h, &h->csr_ptr, ncells + 1, "scatter row pointers")) != MM_OK) return cleanup(), rc;
-    if ((rc = alloc(h, &h->csr_idx, nent, "scatter sample index")) != MM_OK) return cleanup(), rc;
-    if ((rc = alloc(h, &h->csr_w, nent, "scatter weights")) != MM_OK) return cleanup(), rc;
+    if ((rc = dev_alloc((void**)&head, nent * 4, "scatter merge flags")) != MM_OK) return cleanup(), rc;
+    if ((rc = dev_alloc((void**)&pos, nent * 4, "scatter entry positions")) != MM_OK) return cleanup(), rc;
+    cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, kin, kout, (int64_t)nent, 0, 33 + pairbits, st);
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, head, pos, (int64_t)nent, st);
+    tmp_bytes = std::max(tmp_bytes, scan_bytes);
+    if ((rc = dev_alloc(&tmp, tmp_bytes, "sort/scan temp")) != MM_OK) return cleanup(), rc;
     const long gb = (nent + kThreads - 1) / kThreads;
     const float scale = (float)(1.0 / (4.0 * n * (double)n));
-#define MM_K(MM)                                                                                        \
-    case MM:                                                                                            \
-        k_csr_keys<MM><<<gb, kThreads, 0, st>>>(kin, h->d_cos, h->d_sin, n, T, nent);                   \
+#define MM_K(MM)                                                                     \
+    case MM:                                                                         \
+        k_pair_keys<MM><<<gb, kThreads, 0, st>>>(kin, h->d_cos, h->d_sin, n, T, nent); \
         break;
     switch (M) {
         MM_K(2) MM_K(3) MM_K(4) MM_K(5) MM_K(6)
@@ -1195,27 +1247,40 @@ int build_csr(mm_tomo* h, cudaStream_t st) {
 #undef MM_K
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess)
-        e = cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, kin, kout, (int64_t)nent, 0, 32 + cellbits, st);
+        e = cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, kin, kout, (int64_t)nent, 0, 33 + pairbits, st);
     if (e == cudaSuccess) {
-#define MM_P(MM)                                                                                          \
-    case MM:                                                                                              \
-        k_csr_payload<MM><<<gb, kThreads, 0, st>>>(kout, h->csr_idx, h->csr_w, h->d_cos, h->d_sin, n, T, \
-                                                   nent, h->c0, h->c1, scale);                            \
-        break;
-        switch (M) { MM_P(2) MM_P(3) MM_P(4) MM_P(5) MM_P(6) }
-#undef MM_P
-        k_csr_ptr<<<(nent + 1 + kThreads - 1) / kThreads, kThreads, 0, st>>>(kout, h->csr_ptr, nent, ncells);
+#define MM_H(MM) \
+    case MM: k_pair_heads<MM><<<gb, kThreads, 0, st>>>(kout, head, nent); break;
+        switch (M) { MM_H(2) MM_H(3) MM_H(4) MM_H(5) MM_H(6) }
+#undef MM_H
         e = cudaGetLastError();
     }
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, head, pos, (int64_t)nent, st);
+    unsigned last_pos = 0, last_head = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&last_pos, pos + nent - 1, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&last_head, head + nent - 1, 4, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail_cuda(e);
+    const long nnz = (long)last_pos + last_head;
+    if ((rc = alloc(h, &h->csr_ptr, npairs + 1, "scatter pair pointers")) != MM_OK) return cleanup(), rc;
+    if ((rc = alloc(h, &h->csr_idx, nnz, "scatter sample index")) != MM_OK) return cleanup(), rc;
+    if ((rc = alloc(h, &h->csr_w, nnz, "scatter weights")) != MM_OK) return cleanup(), rc;
+    if ((rc = dev_alloc((void**)&pairs, nnz * 4, "scatter entry pairs")) != MM_OK) return cleanup(), rc;
+#define MM_P(MM)                                                                                               \
+    case MM:                                                                                                   \
+        k_pair_payload<MM><<<gb, kThreads, 0, st>>>(kout, head, pos, h->csr_idx, h->csr_w, pairs, h->d_cos,    \
+                                                    h->d_sin, n, T, nent, h->c0, h->c1, scale);                \
+        break;
+    switch (M) { MM_P(2) MM_P(3) MM_P(4) MM_P(5) MM_P(6) }
+#undef MM_P
+    k_pair_ptr<<<(nnz + 1 + kThreads - 1) / kThreads, kThreads, 0, st>>>(pairs, h->csr_ptr, nnz, npairs);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail_cuda(e);
     cleanup();
-    if (e != cudaSuccess) {
-        mm::set_error("building the adjoint scatter table: %s", cudaGetErrorString(e));
-        return MM_ECUDA;
-    }
-    h->nnz = nent;
+    h->nnz = nnz;
     h->csr_ready = true;
-    h->tm.end(st, 3);
+    h->tm.end(st, 4);
     return MM_OK;
 }
 
