@@ -34,6 +34,7 @@ extern "C" {
 
 typedef struct mm_tomo mm_tomo;
 typedef struct mm_prop mm_prop;
+typedef struct mm_fbp mm_fbp;
 
 /* USFFT options.  Zero-initialised fields take the reference defaults
  * (processing/tomo.py:39-42): eps = 1e-3, m from eps (m = 4), oversampling 2. */
@@ -154,6 +155,21 @@ int mm_prop_D_noalloc(int n, int nz, int ntheta, double wavelength, double voxel
 /* Stage timing as for mm_tomo_*_timing.  Stages: 0 y-pass (columns), 1 x-pass (rows). */
 int mm_prop_set_timing(mm_prop* h, int on);
 int mm_prop_get_timing(mm_prop* h, double* ms, long long* calls, int nstages, long long* kernels);
+
+/* ---- FBP filter (step8_fbp path) ----------------------------------------
+ * mm_fbp_create replaces FBPFilter.__init__(n, batch_chunk)
+ *   (processing/fbp_filter.py:41-47).  Rows with 4n a power of two in
+ *   [16, 8192] are filtered in place by one fused kernel without scratch;
+ *   other n use cuFFT over batch_chunk rows at a time. */
+int mm_fbp_create(int n, int batch_chunk, mm_fbp** out);
+int mm_fbp_destroy(mm_fbp* h);
+/* Replaces FBPFilter.filter(sino, w) (processing/fbp_filter.py:128-192): the
+ *   `rows` rows of n float32 samples at `sino` (device) filtered in place with
+ *   the device weights w (2n + 1) of FBPFilter.calc_filter (:49-88, host-side
+ *   FP64 arithmetic, computed by the caller as the reference does):
+ *   edge-replicated padding to 4n, spectrum times w, inverse, centre n kept. */
+int mm_fbp_filter(mm_fbp* h, float* sino, long rows, const float* w, void* stream);
+size_t mm_fbp_workspace_bytes(const mm_fbp* h);
 
 #ifdef __cplusplus
 }
