@@ -35,6 +35,7 @@ extern "C" {
 typedef struct mm_tomo mm_tomo;
 typedef struct mm_prop mm_prop;
 typedef struct mm_fbp mm_fbp;
+typedef struct mm_pgn mm_pgn;
 
 /* USFFT options.  Zero-initialised fields take the reference defaults
  * (processing/tomo.py:39-42): eps = 1e-3, m from eps (m = 4), oversampling 2. */
@@ -170,6 +171,21 @@ int mm_fbp_destroy(mm_fbp* h);
  *   edge-replicated padding to 4n, spectrum times w, inverse, centre n kept. */
 int mm_fbp_filter(mm_fbp* h, float* sino, long rows, const float* w, void* stream);
 size_t mm_fbp_workspace_bytes(const mm_fbp* h);
+
+/* ---- Paganin phase retrieval (step7_paganin path) ------------------------
+ * mm_pgn_create replaces Paganin.__init__(n, nz, ntheta, wavelength,
+ *   voxelsize, distance, alpha) (processing/paganin.py:38-62): filt_host is
+ *   the (nz, n/2 + 1) float32 filter table alpha / (lambda z |k|^2/(4 pi) +
+ *   alpha) on the (fftfreq(nz), rfftfreq(n)) grid, computed by the caller as
+ *   the reference does (:46-53).  n, nz powers of two up to 4096 run three
+ *   fused passes; other sizes cuFFT R2C/C2R over ntheta frames. */
+int mm_pgn_create(int n, int nz, int ntheta, const float* filt_host, mm_pgn** out);
+int mm_pgn_destroy(mm_pgn* h);
+/* Replaces Paganin.retrieve (processing/paganin.py:64-91): frames (<= ntheta)
+ *   of (nz, n) float32 intensity -> -log(clip(irfft2(H rfft2(I)), 1e-6)),
+ *   same shape, into `phase` (device). */
+int mm_pgn_retrieve(mm_pgn* h, const float* intensity, float* phase, int frames, void* stream);
+size_t mm_pgn_workspace_bytes(const mm_pgn* h);
 
 #ifdef __cplusplus
 }
