@@ -411,16 +411,16 @@ def run_tiles(args, local_rank):
 
 # ---------------------------------------------------------------- filtered backprojection (step8)
 def run_fbp(args, local_rank):
-    """step8_fbp's compute (step8_fbp.py:203-205) on the production sinogram:
-    the FBP filter ('shepp', 4x edge padding) of 2058 x 64 rows of 2048, then
-    RT.  Reports the filter alone (rows/s, GB/s of its 8 bytes per sample and
+    """step8_fbp's compute (step8_fbp.py:203-205) on the sinogram of the
+    --base workload (production: 2058 x 64 rows of 2048): the FBP filter
+    ('shepp', 4x edge padding), then RT.  Reports the filter alone (rows/s, GB/s of its 8 bytes per sample and
     the FP32 rate of its two 8192-point transforms per row pair) and the
     filtered backprojection in Gvox*angle/s."""
     import torch
     from model_mosaic_b200.phantom import ellipsoid_volume_torch
     from model_mosaic_b200.processing.fbp_filter import FBPFilter
     from model_mosaic_b200.processing.tomo import TomoReal
-    w = WORKLOADS["production"]
+    w = WORKLOADS[args.base]
     n, nz, T = w["n"], w["nz"], w["ntheta"]
     dev = torch.device("cuda", local_rank)
     theta = np.linspace(0, w["theta_max"], T, endpoint=False).astype(np.float32)
@@ -473,13 +473,13 @@ def run_fbp(args, local_rank):
 
 # ---------------------------------------------------------------- Paganin retrieval (step7)
 def run_paganin(args, local_rank):
-    """step7_paganin's compute on the production frames: Paganin.retrieve of
-    2058 intensity frames of 64 x 2048 (30 keV, 0.12 m, 0.69 um, alpha 1e-3),
-    device-resident.  Three passes of 24 bytes per pixel of HBM traffic
+    """step7_paganin's compute on the frames of the --base workload
+    (production: 2058 intensity frames of 64 x 2048; 30 keV, 0.12 m, 0.69 um,
+    alpha 1e-3), device-resident.  Three passes of 24 bytes per pixel of HBM traffic
     (4 in, 8 + 8 through the half spectrum, 4 out): the roofline is HBM."""
     import torch
     from model_mosaic_b200.processing.paganin import Paganin
-    w = WORKLOADS["production"]
+    w = WORKLOADS[args.base]
     n, nz, T = w["n"], w["nz"], w["ntheta"]
     dev = torch.device("cuda", local_rank)
     pgn = Paganin(n, nz, T, 1.24e-9 / w["energy_kev"], w["voxelsize"], w["distance"], 1e-3)
@@ -647,6 +647,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-rt", action="store_true", help="skip the adjoint (no scatter table)")
     ap.add_argument("--no-model", action="store_true", help="skip the fwd+grad timing of the model")
+    ap.add_argument("--base", choices=sorted(WORKLOADS), default="production",
+                    help="sizes for the fbp and paganin workloads (frames / sinogram of this workload)")
     ap.add_argument("--precision", action="store_true",
                     help="print the precision report (errors vs the FP64 oracle per variant) instead of timing")
     args = ap.parse_args()
