@@ -34,9 +34,13 @@ struct mm_fbp {
 namespace {
 
 // Two rows per block: r0 = 2*blockIdx.x in the real part, r0 + 1 in the
-// imaginary part (zero when absent).
+// imaginary part (zero when absent).  Bounded to 64 registers so that 1024
+// threads share an SM (two 8192-point lines): faster than one block at 128
+// registers despite a few spills.
 template <int L>
-__global__ void __launch_bounds__(stockham::Sched<L>::G) k_fbp_filter(float* __restrict__ rows, long nrows,
+__global__ void __launch_bounds__(stockham::Sched<L>::G,
+                                  stockham::Sched<L>::G >= 32 ? 1024 / stockham::Sched<L>::G : 32)
+    k_fbp_filter(float* __restrict__ rows, long nrows,
                                                                       const float* __restrict__ w,
                                                                       const float2* __restrict__ tw, int n,
                                                                       float inv_ne) {
