@@ -480,10 +480,13 @@ __global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rr2c(const TIN* _
 // The 2m+1 taps of window row v (columns bx .. bx+2m), all loads issued
 // before any is used; taps outside the stored half plane are reflected and
 // conjugated (tap_cell).
-template <int ZV, int M>
-__device__ __forceinline__ void load_row(const float2* __restrict__ F, int bx, int v, bool fast, int n, int zs,
+// ZSC: the slice count zs when fixed at compile time (tap offsets become
+// immediates), 0 for a runtime zs.
+template <int ZV, int M, int ZSC>
+__device__ __forceinline__ void load_row(const float2* __restrict__ F, int bx, int v, bool fast, int n, int zs_rt,
                                          int zoff, float (&val)[2 * M + 1][2 * ZV]) {
     constexpr int L = 2 * M + 1;
+    const int zs = ZSC > 0 ? ZSC : zs_rt;
     const long rowstride = (long)(n + 1) * zs;
     const int twon = 2 * n;
     if (fast) {
@@ -507,7 +510,7 @@ __device__ __forceinline__ void load_row(const float2* __restrict__ F, int bx, i
 }
 
 // Window sum of one sample: (2m+1)^2 taps, row partial sums along x first.
-template <int ZV, int M>
+template <int ZV, int M, int ZSC>
 __device__ __forceinline__ void window_sum(const float2* __restrict__ F, const SampleGeo& g, const float* wx,
                                            const float* wy, float* acc, int n, int zs, int zoff) {
     constexpr int L = 2 * M + 1;
@@ -515,7 +518,7 @@ __device__ __forceinline__ void window_sum(const float2* __restrict__ F, const S
 #pragma unroll
     for (int i1 = 0; i1 < L; ++i1) {
         float val[L][2 * ZV];
-        load_row<ZV, M>(F, g.bx, g.by + i1, fast, n, zs, zoff, val);
+        load_row<ZV, M, ZSC>(F, g.bx, g.by + i1, fast, n, zs, zoff, val);
         float ar[2 * ZV];
 #pragma unroll
         for (int q = 0; q < 2 * ZV; ++q) ar[q] = 0.f;
@@ -545,7 +548,7 @@ __device__ __forceinline__ void store_sample(float2* __restrict__ H, const Sampl
 
 // R stage 5: Gaussian gather of the n/2+1 non-redundant samples per angle.
 // One group of LPS lanes per sample; each lane owns ZV slices.
-template <int ZV, int LPS, int M>
+template <int ZV, int LPS, int M, int ZSC>
 __global__ void __launch_bounds__(kThreads, 3) k_gather(const float2* __restrict__ F, float2* __restrict__ H,
                                                      const float* __restrict__ cosT, const float* __restrict__ sinT,
                                                      int n, int T, int zs, float c0, float c1, float scale,
@@ -575,7 +578,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_gather(const float2* __restrict
     float acc[2 * ZV];
 #pragma unroll
     for (int q = 0; q < 2 * ZV; ++q) acc[q] = 0.f;
-    window_sum<ZV, M>(F, g, wx, wy, acc, n, zs, zoff);
+    window_sum<ZV, M, ZSC>(F, g, wx, wy, acc, n, zs, zoff);
     // k = 0 and k = n/2 are the DC and Nyquist bins of the C2R along r: only
     // their real part enters the result (the .real of tomo.py:150)
     store_sample<ZV>(H, g, acc, k, t, n, T, zs, zoff, scale);
@@ -589,7 +592,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_gather(const float2* __restrict
 // coincide every tap is loaded once and weighted with each sample's own
 // weights, otherwise the two windows are summed one after the other.  Each
 // sample's arithmetic is exactly k_gather's (window_sum, store_sample).
-template <int ZV, int LPS, int M>
+template <int ZV, int LPS, int M, int ZSC>
 __global__ void __launch_bounds__(kThreads, 2) k_gather_pair(const float2* __restrict__ F, float2* __restrict__ H,
                                                           const float* __restrict__ cosT,
                                                           const float* __restrict__ sinT, int n, int T, int zs,
@@ -625,7 +628,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_gather_pair(const float2* __res
 #pragma unroll
         for (int i1 = 0; i1 < L; ++i1) {
             float val[L][2 * ZV];
-            load_row<ZV, M>(F, ga.bx, ga.by + i1, fast, n, zs, zoff, val);
+            load_row<ZV, M, ZSC>(F, ga.bx, ga.by + i1, fast, n, zs, zoff, val);
             float ara[2 * ZV], arb[2 * ZV];
 #pragma unroll
             for (int q = 0; q < 2 * ZV; ++q) ara[q] = arb[q] = 0.f;
@@ -644,8 +647,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_gather_pair(const float2* __res
             }
         }
     } else {
-        window_sum<ZV, M>(F, ga, wxa, wya, acca, n, zs, zoff);
-        window_sum<ZV, M>(F, gb, wxb, wyb, accb, n, zs, zoff);
+        window_sum<ZV, M, ZSC>(F, ga, wxa, wya, acca, n, zs, zoff);
+        window_sum<ZV, M, ZSC>(F, gb, wxb, wyb, accb, n, zs, zoff);
     }
     store_sample<ZV>(H, ga, acca, k, t, n, T, zs, zoff, scale);
     store_sample<ZV>(H, gb, accb, k, t + T2, n, T, zs, zoff, scale);
@@ -1131,7 +1134,7 @@ int pick_lanes(int zs, int& ZV, int& LPS) {
     return MM_OK;
 }
 
-template <int ZV, int LPS>
+template <int ZV, int LPS, int ZSC>
 int launch_gather_m(mm_tomo* h, cudaStream_t st) {
     const int K = h->K;
     const long samples = (long)(h->paired ? h->ntheta / 2 : h->ntheta) * K;  // paired: one lane group per pair
@@ -1141,11 +1144,11 @@ int launch_gather_m(mm_tomo* h, cudaStream_t st) {
 #define MM_G(MM)                                                                                          \
     case MM:                                                                                              \
         if (h->paired)                                                                                    \
-            k_gather_pair<ZV, LPS, MM><<<blocks, kThreads, 0, st>>>(h->F, h->Hh, h->d_cos, h->d_sin, h->n, \
+            k_gather_pair<ZV, LPS, MM, ZSC><<<blocks, kThreads, 0, st>>>(h->F, h->Hh, h->d_cos, h->d_sin, h->n, \
                                                                     h->ntheta, h->zs, h->c0, h->c1, scale, \
                                                                     h->clamp);                              \
         else                                                                                              \
-            k_gather<ZV, LPS, MM><<<blocks, kThreads, 0, st>>>(h->F, h->Hh, h->d_cos, h->d_sin, h->n,      \
+            k_gather<ZV, LPS, MM, ZSC><<<blocks, kThreads, 0, st>>>(h->F, h->Hh, h->d_cos, h->d_sin, h->n, \
                                                                h->ntheta, h->zs, h->c0, h->c1, scale,      \
                                                                h->clamp);                                  \
         break;
@@ -1161,14 +1164,15 @@ int launch_gather_m(mm_tomo* h, cudaStream_t st) {
 int launch_gather(mm_tomo* h, cudaStream_t st) {
     int ZV, LPS;
     pick_lanes(h->zs, ZV, LPS);
-    if (ZV == 1) return launch_gather_m<1, 1>(h, st);
+    if (ZV == 1) return launch_gather_m<1, 1, 0>(h, st);
     switch (LPS) {
-        case 1: return launch_gather_m<2, 1>(h, st);
-        case 2: return launch_gather_m<2, 2>(h, st);
-        case 4: return launch_gather_m<2, 4>(h, st);
-        case 8: return launch_gather_m<2, 8>(h, st);
-        case 16: return launch_gather_m<2, 16>(h, st);
-        default: return launch_gather_m<2, 32>(h, st);
+        case 1: return launch_gather_m<2, 1, 0>(h, st);
+        case 2: return launch_gather_m<2, 2, 0>(h, st);
+        case 4: return launch_gather_m<2, 4, 0>(h, st);
+        case 8: return launch_gather_m<2, 8, 0>(h, st);
+        case 16: return launch_gather_m<2, 16, 0>(h, st);
+        default:  // 64 slices (the production slab) with compile-time tap offsets
+            return h->zs == 64 ? launch_gather_m<2, 32, 64>(h, st) : launch_gather_m<2, 32, 0>(h, st);
     }
 }
 
