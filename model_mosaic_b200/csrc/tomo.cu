@@ -674,12 +674,13 @@ __device__ __forceinline__ void acc_add(float& s, float& c, float w, float v) {
 // each table entry carries the sample's weight for either cell and the
 // sample's spectrum row is loaded once for both.  idx bit 31 / bit 30:
 // conjugate for the left / right cell.
-template <int ZV, int LPS, bool KAHAN>
+template <int ZV, int LPS, bool KAHAN, int ZSC>
 __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict__ ptr,
                                                       const unsigned* __restrict__ idx,
                                                       const float2* __restrict__ wgt,
                                                       const float2* __restrict__ Q, float2* __restrict__ A,
-                                                      long npairs, int zs, int n, int prune) {
+                                                      long npairs, int zs_rt, int n, int prune) {
+    const int zs = ZSC > 0 ? ZSC : zs_rt;  // compile-time slice count: immediate offsets
     constexpr int SPW = 32 / LPS;
     const int lane = threadIdx.x & 31;
     const int sub = lane / LPS, zl = lane % LPS;
@@ -1181,7 +1182,10 @@ int launch_scatter_t(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) {
     const long npairs = 2L * h->n * (h->n / 2 + 1);
     const long warps = ((npairs + (32 / LPS) - 1) / (32 / LPS)) * (h->zs / (LPS * ZV));
     const long blocks = (warps * 32 + kThreads - 1) / kThreads;
-    auto kern = h->compensated ? k_scatter<ZV, LPS, true> : k_scatter<ZV, LPS, false>;
+    auto kern = h->compensated ? k_scatter<ZV, LPS, true, 0> : k_scatter<ZV, LPS, false, 0>;
+    if (ZV == 2 && LPS == 32 && h->zs == 64)  // the production slab: compile-time tap offsets
+        kern = h->compensated ? k_scatter<ZV, LPS, true, (ZV == 2 && LPS == 32) ? 64 : 0>
+                              : k_scatter<ZV, LPS, false, (ZV == 2 && LPS == 32) ? 64 : 0>;
     // the native inverse column transform treats cells beyond radius n + 16
     // as zeros; cuFFT (other sizes) reads them, so they are written then
     const int L = 2 * h->n;
