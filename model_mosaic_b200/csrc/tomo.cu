@@ -238,13 +238,16 @@ __global__ void k_transpose_out(const float2* __restrict__ B, float2* __restrict
 // column are not stored (about a fifth of the half plane).  Inverse: the
 // scatter leaves those cells unwritten (they receive nothing), so they are
 // read as zeros.
-template <int L, bool INV>
+// ZSC: zs fixed at compile time (then the row stride (n+1)*zs is too), 0 for runtime.
+template <int L, bool INV, int ZSC>
 __global__ void __launch_bounds__(4 * stockham::Sched<L>::G) k_col_fft(const float2* __restrict__ src,
                                                                            float2* __restrict__ dst,
                                                                            const float2* __restrict__ tw,
-                                                                           long ncols, int zs) {
+                                                                           long ncols_rt, int zs_rt) {
     namespace sk = stockham;
     constexpr int CW = 4;
+    const int zs = ZSC > 0 ? ZSC : zs_rt;
+    const long ncols = ZSC > 0 ? (long)(L / 2 + 1) * ZSC : ncols_rt;
     extern __shared__ float2 sm[];
     const int c = threadIdx.x, g = threadIdx.y;
     const long col = (long)blockIdx.x * CW + c;
@@ -1002,7 +1005,7 @@ int launch_col_fft_l(mm_tomo* h, const float2* src, float2* dst, cudaStream_t st
     constexpr int CW = 4, G = sk::Sched<L>::G;
     const long ncols = (long)(h->n + 1) * h->zs;
     const size_t smem = (size_t)sk::ColAddr<CW>::rows(L) * CW * sizeof(float2);
-    auto kern = k_col_fft<L, INV>;
+    auto kern = h->zs == 64 ? k_col_fft<L, INV, 64> : k_col_fft<L, INV, 0>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 block(CW, G), grid((unsigned)((ncols + CW - 1) / CW));
     kern<<<grid, block, smem, st>>>(src, dst, h->d_twy, ncols, h->zs);
