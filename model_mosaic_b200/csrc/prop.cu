@@ -82,10 +82,12 @@ __device__ __forceinline__ float2 pair_mix(const float4* __restrict__ S, int k, 
 // IN: 0 complex input, 1 real projection (psi built on load).  Block
 // (CW, G): lanes run over CW adjacent columns, threadIdx.y over the
 // G = nz/16 threads of each column's Stockham transform (fft_smem.cuh).
-template <int N, int CW, int IN>
+// NXC: the row length n fixed at compile time (row offsets become immediates), 0 for runtime.
+template <int N, int CW, int IN, int NXC>
 __global__ void __launch_bounds__(CW * stockham::Sched<N>::G, 1024 / (CW * stockham::Sched<N>::G))
     k_ypass(const void* __restrict__ src, float2* __restrict__ dst, const float4* __restrict__ Sy,
-            const float2* __restrict__ tw, int n, float s, float ib) {
+            const float2* __restrict__ tw, int n_rt, float s, float ib) {
+    const int n = NXC > 0 ? NXC : n_rt;
     extern __shared__ float2 sm[];  // [rows(N)][CW]
     const int c = threadIdx.x, g = threadIdx.y;
     const int x = blockIdx.x * CW + c;
@@ -272,7 +274,7 @@ int launch_y(mm_prop* h, const void* src, int ntheta, const float4* S, float s, 
     constexpr int G = stockham::Sched<N>::G;
     constexpr int CW = y_cols<N>();
     const size_t smem = (size_t)stockham::ColAddr<CW>::rows(N) * CW * sizeof(float2);
-    auto kern = k_ypass<N, CW, IN>;
+    auto kern = h->n == 2048 ? k_ypass<N, CW, IN, 2048> : k_ypass<N, CW, IN, 0>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 block(CW, G), grid((h->n + CW - 1) / CW, ntheta);
     h->tm.begin(0, st);
