@@ -508,6 +508,109 @@ def run_paganin(args, local_rank):
             "config": {"frames": T, "nz": nz, "n": n, "alpha": 1e-3, "data": "synthetic 0.5 + 0.5 U[0, 1)"}}
 
 
+# ---------------------------------------------------------------- mosaic tiles (step4 / step6)
+def run_stitch(args, local_rank):
+    """step6_stitch's blend (step6_stitch.py:206-262) for one vchunk of 64
+    output angles (its default --nthetachunk) on the reference's ups = 2
+    mosaic (6144 x 6144 projection, 11 x 4 tiles of 606 x 808, overlap 50),
+    tiles device-resident; beside it step4_extract's crop (step4_extract.py:
+    176-192) of the same 64 angles.  Algorithmic bytes: every tile frame read
+    once plus the output written once (stitch); every tile pixel read from the
+    projection and written once (extract).  Inputs are 10-11 GB, far above
+    L2.  e2e: the same stitch for 8 angles with the tile frames copied in
+    from pinned host memory and the result copied back inside the timed
+    region.  cpu_baseline: the reference's NumPy blend (oracle/mosaic.py,
+    one thread) on 2 angles of the same mosaic."""
+    import torch
+    from model_mosaic_b200 import mosaic as mo
+    from oracle import mosaic as om
+    dev = torch.device("cuda", local_rank)
+    meta, rows = mo.mosaic_layout(2)
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        mo.write_positions_file(os.path.join(d, "pos.txt"), meta, rows)
+        meta, pl = mo.read_placements(os.path.join(d, "pos.txt"))
+    nth = 64
+    nz, n = meta["NZ"], meta["N"]
+    mt = mo.MosaicTiles(dict(meta, N_HALF=nth, NTHETA=2 * nth), pl)
+    g = torch.Generator(device=dev).manual_seed(0)
+    proj = 0.5 + torch.rand((nth, nz, n), device=dev, generator=g)
+    tiles = mt.extract(proj)  # (2 nth, h, w) per tile: direct then mirror frames
+    for k, t in enumerate(tiles):  # one gain per tile: overlapping tiles disagree as after step5
+        t.mul_(1.0 + 0.01 * k)
+    out = torch.empty_like(proj)
+    st = torch.cuda.current_stream(dev)
+    direct = [t[:nth] for t in tiles]
+    mirror = [t[nth:] for t in tiles]
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / steps
+
+    ms_stitch = timed(lambda: mt.stitch_into(direct, mirror, out), args.steps)
+    ms_extract = timed(lambda: mt.extract_into(proj, direct, mirror), args.steps)
+    tile_px = sum(2 * nth * h * w for h, w in mt.shapes)
+    out_px = nth * nz * n
+    b_stitch = 4 * (tile_px + out_px)
+    b_extract = 8 * tile_px
+    peak, peak_kind = peaks()
+    gbs = b_stitch / (ms_stitch * 1e-3) / 1e9
+    gbs_x = b_extract / (ms_extract * 1e-3) / 1e9
+    del proj
+    # e2e: 8 angles through pinned host memory
+    ne = 8
+    mt8 = mo.MosaicTiles(dict(meta, N_HALF=ne, NTHETA=2 * ne), pl)
+    host_tiles = [torch.cat([t[:ne], t[nth:nth + ne]]).cpu().pin_memory() for t in tiles]
+    del tiles, direct, mirror, out
+    dev_tiles = [torch.empty(t.shape, dtype=torch.float32, device=dev) for t in host_tiles]
+    out8 = torch.empty((ne, nz, n), dtype=torch.float32, device=dev)
+    host_out = torch.empty((ne, nz, n), dtype=torch.float32).pin_memory()
+
+    def e2e():
+        for hsrc, dd in zip(host_tiles, dev_tiles):
+            dd.copy_(hsrc, non_blocking=True)
+        mt8.stitch(dev_tiles, 0, ne, out=out8)
+        host_out.copy_(out8, non_blocking=True)
+
+    ms_e2e = timed(e2e, max(2, args.steps // 2))
+    h2d = sum(t.numel() * 4 for t in host_tiles)
+    # CPU: the reference's NumPy blend on 2 angles of the same mosaic
+    import time
+    s = 2
+    tiles_np = [np.concatenate([t[:s].numpy(), t[ne:ne + s].numpy()]) for t in host_tiles]
+    t0 = time.perf_counter()
+    om.stitch(tiles_np, pl, nz, n, s, meta["OVERLAP"], 0, s)
+    t_cpu = time.perf_counter() - t0
+    mt.free()
+    mt8.free()
+    return {"metric": "mosaic stitch Gpix/s", "workload": "stitch",
+            "value": round(out_px / (ms_stitch * 1e-3) / 1e9, 3), "unit": "Gpix/s",
+            "ms_per_step": round(ms_stitch, 3), "steps": args.steps, "warmup": args.warmup,
+            "roofline": {"bound": "hbm", "kernel": "k_stitch", "achieved": round(gbs, 1), "peak": peak,
+                         "peak_source": peak_kind, "unit": "GB/s", "frac": round(gbs / peak, 4),
+                         "alg_bytes_per_launch": b_stitch},
+            "extract": {"ms": round(ms_extract, 3), "gbs": round(gbs_x, 1), "frac": round(gbs_x / peak, 4),
+                        "alg_bytes_per_launch": b_extract, "kernel": "k_extract"},
+            "e2e": {"value": round(ne * nz * n / (ms_e2e * 1e-3) / 1e9, 3), "unit": "Gpix/s",
+                    "ms_per_step": round(ms_e2e, 3), "angles": ne, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": ne * nz * n * 4},
+            "cpu_baseline": {"value": round(s * nz * n / t_cpu / 1e9, 5), "unit": "Gpix/s", "cores": 1,
+                             "kind": "port", "sample": f"the reference's NumPy blend, {s} output angles"},
+            "gpu_launches": args.steps,
+            "config": {"mosaic": "ups 2: 6144 x 6144, 11 x 4 tiles of 606 x 808, overlap 50", "angles": nth,
+                       "tile_gb": round(4 * tile_px / 1e9, 2), "out_gb": round(4 * out_px / 1e9, 2),
+                       "l2": "inputs far larger than L2; no flush",
+                       "data": "synthetic 0.5 + U[0, 1) projection, per-tile gains 1 + 0.01 k"}}
+
+
 # ---------------------------------------------------------------- precision report
 def run_precision(args, local_rank):
     """Relative L2 error against the FP64 oracle, per precision variant: float32
@@ -643,7 +746,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["tiles", "fbp", "paganin"], default="production")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["tiles", "fbp", "paganin", "stitch"], default="production")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-rt", action="store_true", help="skip the adjoint (no scatter table)")
     ap.add_argument("--no-model", action="store_true", help="skip the fwd+grad timing of the model")
@@ -682,6 +785,10 @@ def main():
     if args.workload == "paganin":
         if rank == 0:
             print(json.dumps(run_paganin(args, local_rank)), flush=True)
+        return
+    if args.workload == "stitch":
+        if rank == 0:
+            print(json.dumps(run_stitch(args, local_rank)), flush=True)
         return
 
     if world > 1:

@@ -187,6 +187,35 @@ int mm_pgn_destroy(mm_pgn* h);
 int mm_pgn_retrieve(mm_pgn* h, const float* intensity, float* phase, int frames, void* stream);
 size_t mm_pgn_workspace_bytes(const mm_pgn* h);
 
+/* ---- Mosaic tiles (step4_extract / step6_stitch path) --------------------
+ * mm_mosaic_create takes the placements of read_placements
+ *   (step4_extract.py:52-118) for a big projection of (nz, n) pixels:
+ *   rects holds n_place rows of 8 ints (r_lo_dir, r_hi_dir, c_lo_dir,
+ *   c_hi_dir, r_lo_mir, r_hi_mir, c_lo_mir, c_hi_mir), in placement order;
+ *   overlap is the positions header's OVERLAP, the tent-weight cap
+ *   (step6_stitch.py:70-81).  Footprints must lie inside (nz, n), direct and
+ *   mirror share rows and width; at most 240 placements and at most 32
+ *   footprints over one pixel. */
+typedef struct mm_mosaic mm_mosaic;
+int mm_mosaic_create(int nz, int n, int n_place, const int* rects, int overlap, mm_mosaic** out);
+int mm_mosaic_destroy(mm_mosaic* h);
+/* Replaces the crop loop of step4_extract.py:176-192 for nth angles: proj
+ *   (nth, nz, n) float32 device; dir[p] and mir[p] (host arrays of n_place
+ *   device pointers) each receive (nth, h_p, w_p) frames: the direct crop and
+ *   the h-flipped mirror crop. */
+int mm_mosaic_extract(mm_mosaic* h, const float* proj, int nth, float* const* dir, float* const* mir,
+                      void* stream);
+/* Replaces the blend loop of step6_stitch.py:206-262 for nth output angles:
+ *   dir[p] / mir[p] point at (nth, h_p, w_p) frames of tile p's direct angles
+ *   and its mirror angles (tile[t] and tile[t + N_HALF]); out (nth, nz, n)
+ *   float32 receives sum(w * direct + w * flip(mirror)) / sum(w), or 1.0
+ *   where no footprint covers the pixel, bit-identical to the reference's
+ *   float32 arithmetic. */
+int mm_mosaic_stitch(mm_mosaic* h, float* const* dir, float* const* mir, int nth, float* out, void* stream);
+/* Coverage cells along rows and columns and the most footprints over one pixel. */
+int mm_mosaic_info(const mm_mosaic* h, int* cells_r, int* cells_c, int* max_cover);
+size_t mm_mosaic_workspace_bytes(const mm_mosaic* h);
+
 #ifdef __cplusplus
 }
 #endif

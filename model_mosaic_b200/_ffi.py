@@ -70,12 +70,21 @@ def _declare(L):
     L.mm_pgn_retrieve.argtypes = [p, p, p, i, p]
     L.mm_pgn_workspace_bytes.argtypes = [p]
     L.mm_pgn_workspace_bytes.restype = sz
+    L.mm_mosaic_create.argtypes = [i, i, i, p, i, C.POINTER(p)]
+    L.mm_mosaic_destroy.argtypes = [p]
+    L.mm_mosaic_extract.argtypes = [p, p, i, p, p, p]
+    L.mm_mosaic_stitch.argtypes = [p, p, p, i, p, p]
+    L.mm_mosaic_info.argtypes = [p, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
+    L.mm_mosaic_workspace_bytes.argtypes = [p]
+    L.mm_mosaic_workspace_bytes.restype = sz
     for name in ("mm_prop_grad_forward", "mm_prop_grad_backward", "mm_prop_D_noalloc",
                  "mm_tomo_set_timing", "mm_tomo_get_timing", "mm_prop_set_timing", "mm_prop_get_timing",
                  "mm_tomo_create", "mm_tomo_destroy", "mm_tomo_R", "mm_tomo_R_ex", "mm_tomo_RT", "mm_tomo_prepare_rt",
                  "mm_prop_create", "mm_prop_destroy", "mm_prop_D", "mm_prop_DT", "mm_prop_intensity",
                  "mm_fbp_create", "mm_fbp_destroy", "mm_fbp_filter",
-                 "mm_pgn_create", "mm_pgn_destroy", "mm_pgn_retrieve"):
+                 "mm_pgn_create", "mm_pgn_destroy", "mm_pgn_retrieve",
+                 "mm_mosaic_create", "mm_mosaic_destroy", "mm_mosaic_extract", "mm_mosaic_stitch",
+                 "mm_mosaic_info"):
         getattr(L, name).restype = i
     return L
 
