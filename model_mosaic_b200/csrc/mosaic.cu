@@ -32,6 +32,7 @@ namespace {
 
 constexpr int kMaxPlace = 240;  // 2 * 240 tile pointers fit the 4 KB parameter space
 constexpr int kThreads = 256;
+constexpr int kAngles = 8;  // angles per batch of loads in the extract and stitch loops
 
 struct Rect {
     int r_lo, h, cd, cm, w;
@@ -75,24 +76,27 @@ __global__ void __launch_bounds__(kThreads) k_extract(const float* __restrict__ 
     const int2 er = __ldg(extrow + blockIdx.x);
     const int p = er.x >> 1, mir = er.x & 1, i = er.y;
     const Rect rc = rect[p];
-    const long fr = (long)rc.h * rc.w;
+    const long fr = (long)rc.h * rc.w, plane = (long)nz * n;
     float* d = dst.p[mir * np + p] + (long)i * rc.w;
     const float* s = proj + (long)(rc.r_lo + i) * n;
-    for (int t = 0; t < nth; ++t) {
-        const float* st = s + (long)t * nz * n;
-        float* dt = d + (long)t * fr;
-        if (mir) {
-            const int c1 = rc.cm + rc.w - 1;
-            for (int j = threadIdx.x; j < rc.w; j += kThreads) dt[j] = __ldg(st + c1 - j);
-        } else {
-            for (int j = threadIdx.x; j < rc.w; j += kThreads) dt[j] = __ldg(st + rc.cd + j);
+    for (int j = threadIdx.x; j < rc.w; j += kThreads) {
+        const float* sj = s + (mir ? rc.cm + rc.w - 1 - j : rc.cd + j);
+        float* dj = d + j;
+        int t = 0;
+        for (; t + kAngles <= nth; t += kAngles) {  // kAngles independent loads in flight
+            float v[kAngles];
+#pragma unroll
+            for (int u = 0; u < kAngles; ++u) v[u] = __ldg(sj + (t + u) * plane);
+#pragma unroll
+            for (int u = 0; u < kAngles; ++u) __stcs(dj + (t + u) * fr, v[u]);
         }
+        for (; t < nth; ++t) __stcs(dj + t * fr, __ldg(sj + t * plane));
     }
 }
 
 // MAXE: bound on the entries of any cell (registers hold one pointer and
-// one weight per entry).
-template <int MAXE>
+// one weight per entry); U: angles whose loads are issued together.
+template <int MAXE, int U>
 __global__ void __launch_bounds__(kThreads) k_stitch(TilePtrs src, float* __restrict__ out,
                                                      const Rect* __restrict__ rect,
                                                      const int* __restrict__ rowcell,
@@ -132,8 +136,26 @@ __global__ void __launch_bounds__(kThreads) k_stitch(TilePtrs src, float* __rest
         return;
     }
     const float inv = __fdiv_rn(1.0f, wsum);
-#pragma unroll 2
-    for (int t = 0; t < nth; ++t) {
+    int t = 0;
+    for (; t + U <= nth; t += U) {
+        float v[U][MAXE];
+#pragma unroll
+        for (int k = 0; k < MAXE; ++k)
+            if (k < ne) {
+#pragma unroll
+                for (int u = 0; u < U; ++u) v[u][k] = __ldg(ptr[k] + u * fs[k]);
+                ptr[k] += U * fs[k];
+            }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            float acc = 0.f;
+#pragma unroll
+            for (int k = 0; k < MAXE; ++k)
+                if (k < ne) acc = __fadd_rn(acc, __fmul_rn(v[u][k], wt[k]));
+            __stcs(o + (t + u) * plane, __fmul_rn(acc, inv));
+        }
+    }
+    for (; t < nth; ++t) {
         float acc = 0.f;
 #pragma unroll
         for (int k = 0; k < MAXE; ++k)
@@ -300,16 +322,16 @@ extern "C" int mm_mosaic_stitch(mm_mosaic* h, float* const* dir, float* const* m
     const long blocks = (long)h->nz * ncb;
     MM_REQUIRE(blocks < (1L << 31), "mm_mosaic_stitch: projection too large for one launch");
     const cudaStream_t st = (cudaStream_t)stream;
-#define MM_S(E)                                                                                                 \
-    k_stitch<E><<<(unsigned)blocks, kThreads, 0, st>>>(tp, out, h->rect, h->rowcell, h->colcell, h->cellptr, \
+#define MM_S(E, U)                                                                                              \
+    k_stitch<E, U><<<(unsigned)blocks, kThreads, 0, st>>>(tp, out, h->rect, h->rowcell, h->colcell, h->cellptr, \
                                                        h->cellent, h->np, h->nz, h->n, h->ncells_c, nth, ncb,  \
                                                        (float)h->cap)
     if (h->max_cover <= 4)
-        MM_S(4);
+        MM_S(4, kAngles);
     else if (h->max_cover <= 8)
-        MM_S(8);
+        MM_S(8, kAngles / 2);
     else
-        MM_S(32);
+        MM_S(32, 1);
 #undef MM_S
     MM_LAUNCHED();
     return MM_OK;

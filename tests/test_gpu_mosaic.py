@@ -78,7 +78,7 @@ def test_full_geometry_extract_and_stitch_bitwise(layout1):
     meta, pl = layout1
     mt = mo.MosaicTiles(meta, pl)
     assert mt.info()[2] <= 4
-    nth = 3
+    nth = 11  # one batch of 8 angles plus 3 more in both kernels
     rng = np.random.default_rng(7)
     data = rng.uniform(0.2, 1.8, (nth, meta["NZ"], meta["N"])).astype(np.float32)
     tiles = mt.extract(torch.from_numpy(data).cuda())
