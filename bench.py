@@ -525,12 +525,12 @@ def run_stitch(args, local_rank):
     from model_mosaic_b200 import mosaic as mo
     from oracle import mosaic as om
     dev = torch.device("cuda", local_rank)
-    meta, rows = mo.mosaic_layout(2)
+    meta, rows = mo.mosaic_layout(args.ups)
     import tempfile
     with tempfile.TemporaryDirectory() as d:
         mo.write_positions_file(os.path.join(d, "pos.txt"), meta, rows)
         meta, pl = mo.read_placements(os.path.join(d, "pos.txt"))
-    nth = 64
+    nth = args.angles
     nz, n = meta["NZ"], meta["N"]
     mt = mo.MosaicTiles(dict(meta, N_HALF=nth, NTHETA=2 * nth), pl)
     g = torch.Generator(device=dev).manual_seed(0)
@@ -605,7 +605,8 @@ def run_stitch(args, local_rank):
             "cpu_baseline": {"value": round(s * nz * n / t_cpu / 1e9, 5), "unit": "Gpix/s", "cores": 1,
                              "kind": "port", "sample": f"the reference's NumPy blend, {s} output angles"},
             "gpu_launches": args.steps,
-            "config": {"mosaic": "ups 2: 6144 x 6144, 11 x 4 tiles of 606 x 808, overlap 50", "angles": nth,
+            "config": {"mosaic": f"ups {args.ups}: {nz} x {n}, {meta['n_z']} x {meta['n_x']} tiles of "
+                                 f"{meta['DET_H']} x {meta['DET_W']}, overlap {meta['OVERLAP']}", "angles": nth,
                        "tile_gb": round(4 * tile_px / 1e9, 2), "out_gb": round(4 * out_px / 1e9, 2),
                        "l2": "inputs far larger than L2; no flush",
                        "data": "synthetic 0.5 + U[0, 1) projection, per-tile gains 1 + 0.01 k"}}
@@ -752,6 +753,8 @@ def main():
     ap.add_argument("--no-model", action="store_true", help="skip the fwd+grad timing of the model")
     ap.add_argument("--base", choices=sorted(WORKLOADS), default="production",
                     help="sizes for the fbp and paganin workloads (frames / sinogram of this workload)")
+    ap.add_argument("--ups", type=int, default=2, help="stitch workload: mosaic of this upsampling factor")
+    ap.add_argument("--angles", type=int, default=64, help="stitch workload: output angles per step (>= 8)")
     ap.add_argument("--precision", action="store_true",
                     help="print the precision report (errors vs the FP64 oracle per variant) instead of timing")
     args = ap.parse_args()
