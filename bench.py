@@ -596,6 +596,7 @@ def run_stitch(args, local_rank):
             "ms_per_step": round(ms_stitch, 3), "steps": args.steps, "warmup": args.warmup,
             "roofline": {"bound": "hbm", "kernel": "k_stitch", "achieved": round(gbs, 1), "peak": peak,
                          "peak_source": peak_kind, "unit": "GB/s", "frac": round(gbs / peak, 4),
+                         "traffic": profile_traffic("stitch", "k_stitch") if (args.ups, nth) == (2, 64) else None,
                          "alg_bytes_per_launch": b_stitch},
             "extract": {"ms": round(ms_extract, 3), "gbs": round(gbs_x, 1), "frac": round(gbs_x / peak, 4),
                         "alg_bytes_per_launch": b_extract, "kernel": "k_extract"},

@@ -114,6 +114,36 @@ __device__ __forceinline__ float tap_weight(int ell, float pos, float inv_twon, 
     return (ell & 1) ? -e : e;
 }
 
+// Weights of one or two samples spread over a warp whose 32 lanes all work on
+// the same sample(s): lane q computes weight q (and q + 32) of the list
+// (wx of a, wy of a, wx of b, wy of b), each 2m+1 long, and every lane reads
+// the list back by shuffles -- the same float values as each lane computing
+// all of them, at one or two exponentials per lane instead of 4(2m+1).
+template <int L, int NS>
+struct WarpWeights {
+    float w0, w1;
+    __device__ __forceinline__ static float one(int q, const SampleGeo& ga, const SampleGeo& gb, float inv_twon,
+                                                float c0, float c1) {
+        const int which = q / L, i = q - which * L;
+        const bool b = which >= 2, y = which & 1;
+        const int base = b ? (y ? gb.by : gb.bx) : (y ? ga.by : ga.bx);
+        const float pos = b ? (y ? gb.y0 : gb.x0) : (y ? ga.y0 : ga.x0);
+        const float v = tap_weight(base + i, pos, inv_twon, c1);
+        return y ? c0 * v : v;
+    }
+    __device__ __forceinline__ WarpWeights(int lane, const SampleGeo& ga, const SampleGeo& gb, float inv_twon,
+                                           float c0, float c1) {
+        constexpr int NW = 2 * NS * L;
+        static_assert(NW <= 64, "weights of at most two rounds of 32 lanes");
+        w0 = one(min(lane, NW - 1), ga, gb, inv_twon, c0, c1);
+        w1 = NW > 32 ? one(min(lane + 32, NW - 1), ga, gb, inv_twon, c0, c1) : 0.f;
+    }
+    // weight q of the list (q a compile-time index after unrolling)
+    __device__ __forceinline__ float get(int q) const {
+        return q < 32 ? __shfl_sync(0xffffffffu, w0, q) : __shfl_sync(0xffffffffu, w1, q - 32);
+    }
+};
+
 // Destination of tap (u, v) in the stored half plane (columns 0..n, rows in
 // raw order): reflected through the origin when u is outside [0, n].
 __device__ __forceinline__ void tap_cell(int u, int v, int n, int& row, int& col, bool& cj) {
@@ -572,10 +602,19 @@ __global__ void __launch_bounds__(kThreads, 3) k_gather(const float2* __restrict
     const SampleGeo g = sample_geo(t, k, n, M, cosT, sinT, clamp != 0);
     const float inv_twon = 1.0f / (float)(2 * n);
     float wx[L], wy[L];
+    if constexpr (LPS == 32) {  // one sample per warp: weights spread over the lanes
+        const WarpWeights<L, 1> ww(lane, g, g, inv_twon, c0, c1);
 #pragma unroll
-    for (int i = 0; i < L; ++i) {
-        wx[i] = tap_weight(g.bx + i, g.x0, inv_twon, c1);
-        wy[i] = c0 * tap_weight(g.by + i, g.y0, inv_twon, c1);
+        for (int i = 0; i < L; ++i) {
+            wx[i] = ww.get(i);
+            wy[i] = ww.get(L + i);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < L; ++i) {
+            wx[i] = tap_weight(g.bx + i, g.x0, inv_twon, c1);
+            wy[i] = c0 * tap_weight(g.by + i, g.y0, inv_twon, c1);
+        }
     }
     const int zoff = (int)zg * (LPS * ZV) + zl * ZV;
     float acc[2 * ZV];
@@ -615,12 +654,23 @@ __global__ void __launch_bounds__(kThreads, 2) k_gather_pair(const float2* __res
     const SampleGeo gb = sample_geo(t + T2, k, n, M, cosT, sinT, clamp != 0);
     const float inv_twon = 1.0f / (float)(2 * n);
     float wxa[L], wya[L], wxb[L], wyb[L];
+    if constexpr (LPS == 32) {  // one pair per warp: weights spread over the lanes
+        const WarpWeights<L, 2> ww(lane, ga, gb, inv_twon, c0, c1);
 #pragma unroll
-    for (int i = 0; i < L; ++i) {
-        wxa[i] = tap_weight(ga.bx + i, ga.x0, inv_twon, c1);
-        wya[i] = c0 * tap_weight(ga.by + i, ga.y0, inv_twon, c1);
-        wxb[i] = tap_weight(gb.bx + i, gb.x0, inv_twon, c1);
-        wyb[i] = c0 * tap_weight(gb.by + i, gb.y0, inv_twon, c1);
+        for (int i = 0; i < L; ++i) {
+            wxa[i] = ww.get(i);
+            wya[i] = ww.get(L + i);
+            wxb[i] = ww.get(2 * L + i);
+            wyb[i] = ww.get(3 * L + i);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < L; ++i) {
+            wxa[i] = tap_weight(ga.bx + i, ga.x0, inv_twon, c1);
+            wya[i] = c0 * tap_weight(ga.by + i, ga.y0, inv_twon, c1);
+            wxb[i] = tap_weight(gb.bx + i, gb.x0, inv_twon, c1);
+            wyb[i] = c0 * tap_weight(gb.by + i, gb.y0, inv_twon, c1);
+        }
     }
     const int zoff = (int)zg * (LPS * ZV) + zl * ZV;
     float acca[2 * ZV], accb[2 * ZV];
