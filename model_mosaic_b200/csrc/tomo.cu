@@ -581,8 +581,17 @@ __device__ __forceinline__ void store_sample(float2* __restrict__ H, const Sampl
 
 // R stage 5: Gaussian gather of the n/2+1 non-redundant samples per angle.
 // One group of LPS lanes per sample; each lane owns ZV slices.
+// Blocks per SM: 4 (64 registers) when the weights are spread over the lanes
+// and the window is at most 9 x 9; else 3 for single samples (a few spills
+// at m >= 4 when several samples share a warp, still faster than 2 blocks)
+// and 2 for pairs.
+template <int LPS, int M, bool PAIR>
+constexpr int gather_min_blocks() {
+    return (LPS == 32 && M <= 4) ? 4 : (PAIR ? 2 : 3);
+}
+
 template <int ZV, int LPS, int M, int ZSC>
-__global__ void __launch_bounds__(kThreads, 3) k_gather(const float2* __restrict__ F, float2* __restrict__ H,
+__global__ void __launch_bounds__(kThreads, gather_min_blocks<LPS, M, false>()) k_gather(const float2* __restrict__ F, float2* __restrict__ H,
                                                      const float* __restrict__ cosT, const float* __restrict__ sinT,
                                                      int n, int T, int zs, float c0, float c1, float scale,
                                                      int clamp) {
@@ -635,7 +644,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_gather(const float2* __restrict
 // weights, otherwise the two windows are summed one after the other.  Each
 // sample's arithmetic is exactly k_gather's (window_sum, store_sample).
 template <int ZV, int LPS, int M, int ZSC>
-__global__ void __launch_bounds__(kThreads, 2) k_gather_pair(const float2* __restrict__ F, float2* __restrict__ H,
+__global__ void __launch_bounds__(kThreads, gather_min_blocks<LPS, M, true>()) k_gather_pair(const float2* __restrict__ F, float2* __restrict__ H,
                                                           const float* __restrict__ cosT,
                                                           const float* __restrict__ sinT, int n, int T, int zs,
                                                           float c0, float c1, float scale, int clamp) {
