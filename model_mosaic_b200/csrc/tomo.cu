@@ -61,6 +61,13 @@ struct mm_tomo {
     unsigned* csr_idx = nullptr;  // sample index (k*T + t) | conj left << 31 | conj right << 30
     float2* csr_w = nullptr;      // (left, right) weights
     size_t nnz = 0;
+    // pairs whose lists exceed kChunk entries (the cells around the spectrum
+    // origin collect thousands) are summed in kChunk-entry pieces by separate
+    // warps and combined in piece order
+    uint2* chunk_task = nullptr;  // (first, end) entry of each piece
+    uint4* chunk_pair = nullptr;  // (pair, first piece, end piece, 0) per long pair
+    float2* chunk_part = nullptr; // (pieces, 2, zs) partial sums: left and right cell
+    long nchunks = 0, nlong = 0;
     float* ypad = nullptr;       // (T, zs, n) real sino padded in z (nz < zs)
     float2* yc = nullptr;        // (T, zs, n) complex sino spectrum (complex RT)
     size_t ws_bytes = 0;
@@ -365,7 +372,7 @@ __global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xfwd(const TIN* _
 // u = 0 and u = n, two rows packed per complex inverse line, crop to
 // [n/2, 3n/2), times phi.  OUT 0: float obj; 1/2: real/imag part of complex.
 template <int L, int OUT, typename TOUT = float>
-__global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xinv(const float2* __restrict__ B,
+__global__ void __launch_bounds__(2 * stockham::Sched<L>::G, 2) k_xinv(const float2* __restrict__ B,
                                                                      void* __restrict__ obj,
                                                                      const float* __restrict__ phi1, float phis,
                                                                      const float2* __restrict__ tw, int nzc,
@@ -431,7 +438,7 @@ __global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xinv(const float2
 // i e^{+2 pi i k/2M} (X[k] - conj X[M-k]); x[2m] = Re z[m], x[2m+1] = Im z[m].
 // Block (G, 8): eight columns (64 bytes per k) per block.
 template <int M, typename TOUT>
-__global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rc2r(const float2* __restrict__ H,
+__global__ void __launch_bounds__(8 * stockham::Sched<M>::G, 2) k_rc2r(const float2* __restrict__ H,
                                                                      TOUT* __restrict__ out,
                                                                      const float2* __restrict__ tw,
                                                                      const float2* __restrict__ ex, long C) {
@@ -730,40 +737,14 @@ __device__ __forceinline__ void acc_add(float& s, float& c, float w, float v) {
     }
 }
 
-// RT: pull-scatter over the static pair table.  One lane group per pair of
-// horizontally adjacent cells (row, 2p) and (row, 2p+1): the two cells
-// receive almost the same samples (8 of a window's 9 columns cover both), so
-// each table entry carries the sample's weight for either cell and the
-// sample's spectrum row is loaded once for both.  idx bit 31 / bit 30:
-// conjugate for the left / right cell.
-template <int ZV, int LPS, bool KAHAN, int ZSC>
-__global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict__ ptr,
-                                                      const unsigned* __restrict__ idx,
-                                                      const float2* __restrict__ wgt,
-                                                      const float2* __restrict__ Q, float2* __restrict__ A,
-                                                      long npairs, int zs_rt, int n, int prune) {
-    const int zs = ZSC > 0 ? ZSC : zs_rt;  // compile-time slice count: immediate offsets
-    constexpr int SPW = 32 / LPS;
-    const int lane = threadIdx.x & 31;
-    const int sub = lane / LPS, zl = lane % LPS;
-    const int zgroups = zs / (LPS * ZV);
-    const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long zg = warp % zgroups;
-    const long p = (warp / zgroups) * SPW + sub;
-    if (p >= npairs) return;
-    const int NP = n / 2 + 1;
-    const int row = (int)(p / NP), c0 = (int)(p % NP) * 2;
-    // cells beyond radius n + 16 receive nothing; with `prune` they are not
-    // written (k_col_fft reads them as zeros)
-    const int vw = row < n ? row : row - 2 * n;
-    const int lim = (n + 16) * (n + 16) - vw * vw;
-    const bool keepL = !prune || c0 * c0 <= lim;
-    const bool keepR = c0 + 1 <= n && (!prune || (c0 + 1) * (c0 + 1) <= lim);
-    if (!keepL && !keepR) return;
-    const int zoff = (int)zg * (LPS * ZV) + zl * ZV;
-    float al[2 * ZV], cl[2 * ZV], ar[2 * ZV], cr[2 * ZV];
-#pragma unroll
-    for (int q = 0; q < 2 * ZV; ++q) al[q] = cl[q] = ar[q] = cr[q] = 0.f;
+constexpr unsigned kChunk = 256;  // longest list one lane group sums alone
+
+// Sums of the table entries [e0, e1) of one cell pair, left cell in al
+// (compensation cl), right cell in ar (cr).
+template <int ZV, int LPS, bool KAHAN>
+__device__ __forceinline__ void pair_sums(unsigned e0, unsigned e1, const unsigned* __restrict__ idx,
+                                          const float2* __restrict__ wgt, const float2* __restrict__ Q, int zs,
+                                          int zoff, int lane, float* al, float* cl, float* ar, float* cr) {
     auto add = [&](unsigned ii, float2 w, const float* v) {
         const float sl = (ii >> 31) ? -w.x : w.x, sr = ((ii >> 30) & 1u) ? -w.y : w.y;
 #pragma unroll
@@ -774,7 +755,6 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict
             acc_add<KAHAN>(ar[q + 1], cr[q + 1], sr, v[q + 1]);
         }
     };
-    const unsigned e0 = __ldg(ptr + p), e1 = __ldg(ptr + p + 1);
     if constexpr (LPS == 32) {
         // one pair per warp: 32 table entries per coalesced load, handed out
         // by shuffles, four independent spectrum loads in flight
@@ -832,9 +812,124 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict
             add(ia, wa, va);
         }
     }
-    const long cell = (long)row * (n + 1) + c0;
-    if (keepL) ZVec<ZV>::store(A + cell * zs + zoff, al);
-    if (keepR) ZVec<ZV>::store(A + (cell + 1) * zs + zoff, ar);
+}
+
+// Destination cells of pair p; cells beyond radius n + 16 receive nothing
+// and with `prune` are not written (k_col_fft reads them as zeros).
+struct PairCells {
+    long cell;
+    bool keepL, keepR;
+    __device__ __forceinline__ PairCells(long p, int n, int prune) {
+        const int NP = n / 2 + 1;
+        const int row = (int)(p / NP), c0 = (int)(p % NP) * 2;
+        const int vw = row < n ? row : row - 2 * n;
+        const int lim = (n + 16) * (n + 16) - vw * vw;
+        keepL = !prune || c0 * c0 <= lim;
+        keepR = c0 + 1 <= n && (!prune || (c0 + 1) * (c0 + 1) <= lim);
+        cell = (long)row * (n + 1) + c0;
+    }
+};
+
+// One lane group per (pair or piece, slice group): the warp decomposition
+// shared by the three scatter kernels.
+template <int ZV, int LPS>
+struct ScatterLanes {
+    int lane, zoff;
+    long item;
+    __device__ __forceinline__ ScatterLanes(int zs) {
+        constexpr int SPW = 32 / LPS;
+        lane = threadIdx.x & 31;
+        const int sub = lane / LPS, zl = lane % LPS;
+        const int zgroups = zs / (LPS * ZV);
+        const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        item = (warp / zgroups) * SPW + sub;
+        zoff = (int)(warp % zgroups) * (LPS * ZV) + zl * ZV;
+    }
+};
+
+// RT: pull-scatter over the static pair table.  One lane group per pair of
+// horizontally adjacent cells (row, 2p) and (row, 2p+1): the two cells
+// receive almost the same samples (8 of a window's 9 columns cover both), so
+// each table entry carries the sample's weight for either cell and the
+// sample's spectrum row is loaded once for both.  idx bit 31 / bit 30:
+// conjugate for the left / right cell.  Pairs with more than kChunk entries
+// are left to k_scatter_pieces / k_scatter_combine.
+template <int ZV, int LPS, bool KAHAN, int ZSC>
+__global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict__ ptr,
+                                                      const unsigned* __restrict__ idx,
+                                                      const float2* __restrict__ wgt,
+                                                      const float2* __restrict__ Q, float2* __restrict__ A,
+                                                      long npairs, int zs_rt, int n, int prune) {
+    const int zs = ZSC > 0 ? ZSC : zs_rt;  // compile-time slice count: immediate offsets
+    const ScatterLanes<ZV, LPS> ln(zs);
+    const long p = ln.item;
+    if (p >= npairs) return;
+    const PairCells pc(p, n, prune);
+    if (!pc.keepL && !pc.keepR) return;
+    const unsigned e0 = __ldg(ptr + p), e1 = __ldg(ptr + p + 1);
+    if (e1 - e0 > kChunk) return;
+    float al[2 * ZV], cl[2 * ZV], ar[2 * ZV], cr[2 * ZV];
+#pragma unroll
+    for (int q = 0; q < 2 * ZV; ++q) al[q] = cl[q] = ar[q] = cr[q] = 0.f;
+    pair_sums<ZV, LPS, KAHAN>(e0, e1, idx, wgt, Q, zs, ln.zoff, ln.lane, al, cl, ar, cr);
+    if (pc.keepL) ZVec<ZV>::store(A + pc.cell * zs + ln.zoff, al);
+    if (pc.keepR) ZVec<ZV>::store(A + (pc.cell + 1) * zs + ln.zoff, ar);
+}
+
+// Pieces of the long lists: partial sums of kChunk entries each.  With
+// KAHAN the partial is the compensated sum s - c.
+template <int ZV, int LPS, bool KAHAN, int ZSC>
+__global__ void __launch_bounds__(kThreads) k_scatter_pieces(const uint2* __restrict__ task,
+                                                             const unsigned* __restrict__ idx,
+                                                             const float2* __restrict__ wgt,
+                                                             const float2* __restrict__ Q,
+                                                             float2* __restrict__ part, long ntasks, int zs_rt) {
+    const int zs = ZSC > 0 ? ZSC : zs_rt;
+    const ScatterLanes<ZV, LPS> ln(zs);
+    if (ln.item >= ntasks) return;
+    const uint2 tk = __ldg(task + ln.item);
+    float al[2 * ZV], cl[2 * ZV], ar[2 * ZV], cr[2 * ZV];
+#pragma unroll
+    for (int q = 0; q < 2 * ZV; ++q) al[q] = cl[q] = ar[q] = cr[q] = 0.f;
+    pair_sums<ZV, LPS, KAHAN>(tk.x, tk.y, idx, wgt, Q, zs, ln.zoff, ln.lane, al, cl, ar, cr);
+    if constexpr (KAHAN) {
+#pragma unroll
+        for (int q = 0; q < 2 * ZV; ++q) {
+            al[q] -= cl[q];
+            ar[q] -= cr[q];
+        }
+    }
+    ZVec<ZV>::store(part + (2 * ln.item) * zs + ln.zoff, al);
+    ZVec<ZV>::store(part + (2 * ln.item + 1) * zs + ln.zoff, ar);
+}
+
+// Long pairs: their pieces' partial sums added in piece order.
+template <int ZV, int LPS, bool KAHAN, int ZSC>
+__global__ void __launch_bounds__(kThreads) k_scatter_combine(const uint4* __restrict__ lp,
+                                                              const float2* __restrict__ part,
+                                                              float2* __restrict__ A, long nlong, int zs_rt, int n,
+                                                              int prune) {
+    const int zs = ZSC > 0 ? ZSC : zs_rt;
+    const ScatterLanes<ZV, LPS> ln(zs);
+    if (ln.item >= nlong) return;
+    const uint4 q4 = __ldg(lp + ln.item);
+    const PairCells pc((long)q4.x, n, prune);
+    if (!pc.keepL && !pc.keepR) return;
+    float al[2 * ZV], cl[2 * ZV], ar[2 * ZV], cr[2 * ZV];
+#pragma unroll
+    for (int q = 0; q < 2 * ZV; ++q) al[q] = cl[q] = ar[q] = cr[q] = 0.f;
+    for (unsigned t = q4.y; t < q4.z; ++t) {
+        float vl[2 * ZV], vr[2 * ZV];
+        ZVec<ZV>::load(part + (2L * t) * zs + ln.zoff, vl);
+        ZVec<ZV>::load(part + (2L * t + 1) * zs + ln.zoff, vr);
+#pragma unroll
+        for (int q = 0; q < 2 * ZV; ++q) {
+            acc_add<KAHAN>(al[q], cl[q], 1.0f, vl[q]);
+            acc_add<KAHAN>(ar[q], cr[q], 1.0f, vr[q]);
+        }
+    }
+    if (pc.keepL) ZVec<ZV>::store(A + pc.cell * zs + ln.zoff, al);
+    if (pc.keepR) ZVec<ZV>::store(A + (pc.cell + 1) * zs + ln.zoff, ar);
 }
 
 // Scatter-table construction ---------------------------------------------
@@ -1244,16 +1339,33 @@ int launch_scatter_t(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) {
     const long npairs = 2L * h->n * (h->n / 2 + 1);
     const long warps = ((npairs + (32 / LPS) - 1) / (32 / LPS)) * (h->zs / (LPS * ZV));
     const long blocks = (warps * 32 + kThreads - 1) / kThreads;
-    auto kern = h->compensated ? k_scatter<ZV, LPS, true, 0> : k_scatter<ZV, LPS, false, 0>;
-    if (ZV == 2 && LPS == 32 && h->zs == 64)  // the production slab: compile-time tap offsets
-        kern = h->compensated ? k_scatter<ZV, LPS, true, (ZV == 2 && LPS == 32) ? 64 : 0>
-                              : k_scatter<ZV, LPS, false, (ZV == 2 && LPS == 32) ? 64 : 0>;
+    constexpr int Z64 = (ZV == 2 && LPS == 32) ? 64 : 0;  // the production slab: compile-time tap offsets
+    const bool z64 = Z64 > 0 && h->zs == 64, kh = h->compensated != 0;
+    auto kern = kh ? (z64 ? k_scatter<ZV, LPS, true, Z64> : k_scatter<ZV, LPS, true, 0>)
+                   : (z64 ? k_scatter<ZV, LPS, false, Z64> : k_scatter<ZV, LPS, false, 0>);
     // the native inverse column transform treats cells beyond radius n + 16
     // as zeros; cuFFT (other sizes) reads them, so they are written then
     const int L = 2 * h->n;
     const int prune = (mm_is_pow2(L) && L >= 16 && L <= 4096) ? 1 : 0;
+    auto grid = [&](long items) {
+        const long w = ((items + (32 / LPS) - 1) / (32 / LPS)) * (h->zs / (LPS * ZV));
+        return (unsigned)((w * 32 + kThreads - 1) / kThreads);
+    };
+    if (h->nchunks > 0) {  // the long lists' pieces first: they are the longest chains
+        auto kp = kh ? (z64 ? k_scatter_pieces<ZV, LPS, true, Z64> : k_scatter_pieces<ZV, LPS, true, 0>)
+                     : (z64 ? k_scatter_pieces<ZV, LPS, false, Z64> : k_scatter_pieces<ZV, LPS, false, 0>);
+        kp<<<grid(h->nchunks), kThreads, 0, st>>>(h->chunk_task, h->csr_idx, h->csr_w, Q, h->chunk_part,
+                                                  h->nchunks, h->zs);
+        MM_LAUNCHED();
+    }
     kern<<<blocks, kThreads, 0, st>>>(h->csr_ptr, h->csr_idx, h->csr_w, Q, A, npairs, h->zs, h->n, prune);
     MM_LAUNCHED();
+    if (h->nlong > 0) {
+        auto kc = kh ? (z64 ? k_scatter_combine<ZV, LPS, true, Z64> : k_scatter_combine<ZV, LPS, true, 0>)
+                     : (z64 ? k_scatter_combine<ZV, LPS, false, Z64> : k_scatter_combine<ZV, LPS, false, 0>);
+        kc<<<grid(h->nlong), kThreads, 0, st>>>(h->chunk_pair, h->chunk_part, A, h->nlong, h->zs, h->n, prune);
+        MM_LAUNCHED();
+    }
     return MM_OK;
 }
 
@@ -1348,6 +1460,27 @@ int build_csr(mm_tomo* h, cudaStream_t st) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail_cuda(e);
     cleanup();
+    // long lists -> pieces of kChunk entries (fixed split: deterministic)
+    std::vector<unsigned> hp(npairs + 1);
+    MM_CUDA(cudaMemcpy(hp.data(), h->csr_ptr, hp.size() * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    std::vector<uint2> tasks;
+    std::vector<uint4> longp;
+    for (long q = 0; q < npairs; ++q) {
+        const unsigned a = hp[q], b = hp[q + 1];
+        if (b - a <= kChunk) continue;
+        const unsigned t0 = (unsigned)tasks.size();
+        for (unsigned x = a; x < b; x += kChunk) tasks.push_back(make_uint2(x, std::min(b, x + kChunk)));
+        longp.push_back(make_uint4((unsigned)q, t0, (unsigned)tasks.size(), 0u));
+    }
+    if (!longp.empty()) {
+        MM_TRY(alloc(h, &h->chunk_task, tasks.size(), "scatter pieces"));
+        MM_TRY(alloc(h, &h->chunk_pair, longp.size(), "scatter long pairs"));
+        MM_TRY(alloc(h, &h->chunk_part, tasks.size() * 2 * (size_t)h->zs, "scatter partial sums"));
+        MM_CUDA(cudaMemcpy(h->chunk_task, tasks.data(), tasks.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+        MM_CUDA(cudaMemcpy(h->chunk_pair, longp.data(), longp.size() * sizeof(uint4), cudaMemcpyHostToDevice));
+    }
+    h->nchunks = (long)tasks.size();
+    h->nlong = (long)longp.size();
     h->nnz = nnz;
     h->csr_ready = true;
     h->tm.end(st, 4);
@@ -1374,7 +1507,7 @@ void destroy(mm_tomo* h) {
     for (cufftHandle p : all)
         if (p) cufftDestroy(p);
     void* bufs[] = {h->d_cos, h->d_sin, h->d_phi1, h->d_twy, h->d_twr, h->d_exr, h->P, h->X, h->Y, h->F, h->Hh, h->sino_tmp, h->fft_work,
-                    h->csr_ptr, h->csr_idx, h->csr_w, h->ypad, h->yc};
+                    h->csr_ptr, h->csr_idx, h->csr_w, h->chunk_task, h->chunk_pair, h->chunk_part, h->ypad, h->yc};
     for (void* b : bufs)
         if (b) cudaFree(b);
     delete h;
@@ -1607,7 +1740,7 @@ int rt_tail(mm_tomo* h, cudaStream_t st) {
     const int n = h->n, zs = h->zs;
     h->tm.begin(7, st);
     MM_TRY(launch_scatter(h, h->Hh, h->F, st));
-    h->tm.end(st, 1);
+    h->tm.end(st, 1 + (h->nchunks > 0) + (h->nlong > 0));
     h->tm.begin(8, st);
     int rc = launch_col_fft<true>(h, h->F, h->Y, st);
     if (rc == -100) {
