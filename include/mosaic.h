@@ -144,12 +144,16 @@ int mm_prop_grad_backward(mm_prop* h, const void* gu, const float* proj, float i
  *   while they run (their GPU memory is reserved up front by their own pool
  *   allocator, so a cudaMalloc mid-run fails or stalls other work).  No
  *   counterpart in the reference.  Same operator and layouts as mm_prop_D for
- *   one distance, without a handle: the chirp/twiddle tables and the
- *   intermediate live in one static 64 MiB device array per GPU, so
- *   (ntheta*nz*n + 8*(n+nz)) * 8 bytes must fit in 64 MiB (MM_EINVAL
- *   otherwise).  The first call on each device resolves that array's address;
- *   make it before any stream capture.  Calls share the array: calls that
- *   overlap on the GPU race and must be ordered by the caller. */
+ *   one distance, without a handle, for n and nz powers of two in [2, 2048]
+ *   (the fused two-pass kernels; mm_prop_D also takes other sizes): the
+ *   chirp/twiddle tables and the intermediate live in one static 64 MiB
+ *   device array per GPU, so (ntheta*nz*n + 8*(n+nz)) * 8 bytes must fit in
+ *   64 MiB (MM_EINVAL otherwise).  CUDA loads device code lazily, so the
+ *   first call on each device is what loads this code and takes the 64 MiB
+ *   (kept until the process exits) and resolves the array's address: make
+ *   one call on each device before reserving a device memory pool and before
+ *   any stream capture.  Calls share the array: calls that overlap on the GPU
+ *   race and must be ordered by the caller. */
 int mm_prop_D_noalloc(int n, int nz, int ntheta, double wavelength, double voxelsize, double distance,
                       const void* psi, void* out, void* stream);
 

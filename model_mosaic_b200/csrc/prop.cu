@@ -276,11 +276,20 @@ int launch_y(mm_prop* h, const void* src, int ntheta, const float4* S, float s, 
     const size_t smem = (size_t)stockham::ColAddr<CW>::rows(N) * CW * sizeof(float2);
     auto kern = h->n == 2048 ? k_ypass<N, CW, IN, 2048> : k_ypass<N, CW, IN, 0>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 block(CW, G), grid((h->n + CW - 1) / CW, ntheta);
+    // one frame per grid row: frames go in launches of at most 65535 (the grid's y limit)
+    const size_t esz = IN == 0 ? sizeof(float2) : sizeof(float);
+    const long frame = (long)N * h->n;
+    int launches = 0;
     h->tm.begin(0, st);
-    kern<<<grid, block, smem, st>>>(src, h->mid, S, h->twy, h->n, s, ib);
-    MM_LAUNCHED();
-    h->tm.end(st, 1);
+    for (int t0 = 0; t0 < ntheta; t0 += 65535) {
+        const int nt = ntheta - t0 < 65535 ? ntheta - t0 : 65535;
+        dim3 block(CW, G), grid((h->n + CW - 1) / CW, nt);
+        kern<<<grid, block, smem, st>>>(static_cast<const char*>(src) + (size_t)t0 * frame * esz,
+                                        h->mid + (size_t)t0 * frame, S, h->twy, h->n, s, ib);
+        MM_LAUNCHED();
+        ++launches;
+    }
+    h->tm.end(st, launches);
     return MM_OK;
 }
 
@@ -562,12 +571,18 @@ extern "C" int mm_prop_get_timing(mm_prop* h, double* ms, long long* calls, int 
 // or stall other work once it is running.  mm_prop_D_noalloc serves them: it
 // takes no handle and calls no cudaMalloc/cudaFree or allocating library
 // routine.  Its working memory -- the chirp and twiddle tables and the
-// column-pass intermediate -- lives in the file-scope array below, which
-// every GPU that loads this library holds (kNoAllocBytes) until the process
-// exits.  All calls share that one array and it keeps the last call's
-// contents, so calls that overlap on the GPU (two streams, two host threads)
-// race; callers must order them.  Nothing in it needs to start at zero: every
-// call rewrites the tables and the intermediate before reading them.
+// column-pass intermediate -- lives in the file-scope array below.  CUDA
+// loads a library's device code lazily by default (CUDA_MODULE_LOADING=LAZY
+// since 12.2), so a GPU takes the array's kNoAllocBytes when this file's
+// device code is first loaded there -- at the latest in the first call's
+// cudaGetSymbolAddress -- and keeps them until the process exits.  A caller
+// that reserves its device memory pool up front must therefore make one call
+// (any valid size) on each device before reserving the pool, and before any
+// stream capture.  All calls share that one array and it keeps the last
+// call's contents, so calls that overlap on the GPU (two streams, two host
+// threads) race; callers must order them.  Nothing in it needs to start at
+// zero: every call rewrites the tables and the intermediate before reading
+// them.
 static constexpr size_t kNoAllocBytes = 64ull << 20;  // 64 MiB per device
 static __device__ __align__(256) float2 g_noalloc_scratch[kNoAllocBytes / sizeof(float2)];
 

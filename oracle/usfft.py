@@ -87,11 +87,29 @@ def _window(n, m, mu, x0, y0, dtype):
     return ell0, ell1, ex, ey
 
 
-def gather_rfft_full(fde, theta, n, m, mu, dtype=np.float64, clamp=False, zchunk=8):
+def gather_rfft_full(fde, theta, n, m, mu, dtype=np.float64, clamp=False, zchunk=8, tchunk=None):
     """Polar gather from the (nz, 2n, n+1) raw-order rfft2 half spectrum with
     conjugate reflection for k0 > n and the (-1)^(k0+k1) sign; divides by n.
     processing/kernels.py:274-349 (clamp=True: kernels.py:451-526).
-    Returns g with shape (ntheta, nz, n)."""
+    Returns g with shape (ntheta, nz, n).  Angles are taken `tchunk` at a
+    time (default: enough to keep each index array near 2^23 taps), which
+    bounds the memory at production sizes; the arithmetic per sample is the
+    same whatever the chunking."""
+    ct = _ctype(dtype)
+    nz = fde.shape[0]
+    T = len(theta)
+    L = 2 * m + 1
+    if tchunk is None:
+        tchunk = max(1, (1 << 23) // (n * L * L))
+    g = np.empty((T, nz, n), dtype=ct)
+    fde = fde.astype(ct, copy=False)
+    for t0 in range(0, T, tchunk):
+        t1 = min(T, t0 + tchunk)
+        g[t0:t1] = _gather_angles(fde, np.asarray(theta)[t0:t1], n, m, mu, dtype, clamp, zchunk)
+    return g
+
+
+def _gather_angles(fde, theta, n, m, mu, dtype, clamp, zchunk):
     ct = _ctype(dtype)
     nz = fde.shape[0]
     T = len(theta)
@@ -107,7 +125,6 @@ def gather_rfft_full(fde, theta, n, m, mu, dtype=np.float64, clamp=False, zchunk
     rky = np.where(refl, np.mod(twon - ky, twon), ky)
     sw = (sign * w).astype(dtype)
     g = np.empty((T, nz, n), dtype=ct)
-    fde = fde.astype(ct, copy=False)
     for z0 in range(0, nz, zchunk):
         z1 = min(nz, z0 + zchunk)
         v = fde[z0:z1][:, rky, rkx]                      # (zc, T, n, L, L)
@@ -117,27 +134,35 @@ def gather_rfft_full(fde, theta, n, m, mu, dtype=np.float64, clamp=False, zchunk
     return g
 
 
-def scatter_full(g, theta, n, m, mu, dtype=np.float64):
+def scatter_full(g, theta, n, m, mu, dtype=np.float64, tchunk=None):
     """Adjoint scatter of the full-complex gather kernel (dir=1): every
     sample adds w * g into f[(n + ell1) % 2n, (n + ell0) % 2n]; no divide by n.
-    processing/kernels.py:16-93.  g: (ntheta, nz, n) -> f: (nz, 2n, 2n)."""
+    processing/kernels.py:16-93.  g: (ntheta, nz, n) -> f: (nz, 2n, 2n).
+    Angles are summed `tchunk` at a time into float64 accumulators (the
+    reference's float atomics have no fixed order, so neither does this)."""
     ct = _ctype(dtype)
     T, nz, _ = g.shape
     twon = 2 * n
-    x0, y0 = _polar(n, theta, dtype)
-    ell0, ell1, ex, ey = _window(n, m, mu, x0, y0, dtype)
-    w = (ex[:, :, None, :] * ey[:, :, :, None]).astype(dtype)   # ex[i0]*ey (kernels.py:68)
-    fy = np.mod(n + ell1, twon)[:, :, :, None]
-    fx = np.mod(n + ell0, twon)[:, :, None, :]
-    idx = np.broadcast_to(fy * twon + fx, w.shape).reshape(-1)
-    wf = w.reshape(T, n, -1)
-    out = np.zeros((nz, twon, twon), dtype=ct)
-    for z in range(nz):
-        val = (wf * g[:, z, :, None]).reshape(-1)
-        re = np.bincount(idx, weights=val.real.astype(np.float64), minlength=twon * twon)
-        im = np.bincount(idx, weights=val.imag.astype(np.float64), minlength=twon * twon)
-        out[z] = (re + 1j * im).reshape(twon, twon).astype(ct)
-    return out
+    L = 2 * m + 1
+    if tchunk is None:
+        tchunk = max(1, (1 << 23) // (n * L * L))
+    re = np.zeros((nz, twon * twon), dtype=np.float64)
+    im = np.zeros((nz, twon * twon), dtype=np.float64)
+    th = np.asarray(theta)
+    for t0 in range(0, T, tchunk):
+        t1 = min(T, t0 + tchunk)
+        x0, y0 = _polar(n, th[t0:t1], dtype)
+        ell0, ell1, ex, ey = _window(n, m, mu, x0, y0, dtype)
+        w = (ex[:, :, None, :] * ey[:, :, :, None]).astype(dtype)   # ex[i0]*ey (kernels.py:68)
+        fy = np.mod(n + ell1, twon)[:, :, :, None]
+        fx = np.mod(n + ell0, twon)[:, :, None, :]
+        idx = np.broadcast_to(fy * twon + fx, w.shape).reshape(-1)
+        wf = w.reshape(t1 - t0, n, -1)
+        for z in range(nz):
+            val = (wf * g[t0:t1, z, :, None]).reshape(-1)
+            re[z] += np.bincount(idx, weights=val.real.astype(np.float64), minlength=twon * twon)
+            im[z] += np.bincount(idx, weights=val.imag.astype(np.float64), minlength=twon * twon)
+    return (re + 1j * im).reshape(nz, twon, twon).astype(ct)
 
 
 class TomoRealOracle:
