@@ -45,6 +45,9 @@ WORKLOADS = {
     # same kernels as "production" on a few GB of device memory (for ncu captures)
     "profile": dict(n=1024, nz=64, ntheta=512, theta_max=2 * np.pi, energy_kev=30.0,
                     distance=0.12, voxelsize=0.69e-6),
+    # the production slice size (4096-point columns, 2048-point rows) on ~4.5 GB
+    "profile2048": dict(n=2048, nz=32, ntheta=128, theta_max=2 * np.pi, energy_kev=30.0,
+                        distance=0.12, voxelsize=0.69e-6),
 }
 BETA_RATIO = 100.0
 L2_BYTES = 126 * 2 ** 20
@@ -352,6 +355,32 @@ def run_model(args, local_rank):
         torch.cuda.synchronize()
         out[name + "_ms"] = round(e0.elapsed_time(e1) / args.steps, 3)
     out["speedup_vs_plain"] = round(out["plain_ms"] / out["fused_ms"], 3)
+    # baseline leg: the same step composed from the reference's own kernels
+    # (oracle/refgpu.py: its R, D, psi, |.|^2 plus the exact adjoints)
+    from oracle import refgpu
+    if not args.no_ref_gpu and refgpu.available():
+        inv_norm = m.s      # the model's phase scale s
+        rt = refgpu.RefGpuTomoReal(n, nz, theta, device=dev)
+        rp = refgpu.RefGpuPropagation(n, nz, MODEL["chunk"], 1, 1.24e-9 / w["energy_kev"], w["voxelsize"],
+                                      [w["distance"]], device=dev)
+        ref_step = lambda: refgpu.ref_loss_and_grad(rt, rp, delta, data, inv_norm, 1.0 / BETA_RATIO,  # noqa: E731
+                                                    chunk=MODEL["chunk"])
+        ref_step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(2, min(args.steps, 5))
+        e0.record(st)
+        for _ in range(reps):
+            ref_step()
+        e1.record(st)
+        torch.cuda.synchronize()
+        out["reference_ms"] = round(e0.elapsed_time(e1) / reps, 3)
+        out["speedup_vs_reference"] = round(out["reference_ms"] / out["fused_ms"], 3)
+        out["reference"] = ("the same loss and gradient composed from the reference's kernels "
+                            "(processing/kernels.py for sm_100a) and its cupy glue on torch/cuFFT, with the "
+                            "exact adjoint of its D; atomic scatter in RT")
+        del rt, rp
+        torch.cuda.empty_cache()
     out["config"] = f"{nz} slices of {n}^2, {T} angles on [0, pi), psi recomputed per {MODEL['chunk']}-angle chunk"
     return out
 
@@ -686,6 +715,55 @@ def run_precision(args, local_rank):
                                            "D and the gradient kernels take float32 only"}}
 
 
+# ---------------------------------------------------------------- GPU (reference kernels on this GPU)
+def ref_gpu_ops(args, w, local_rank):
+    """Baseline leg: the reference's own CUDA kernels (processing/kernels.py,
+    compiled verbatim for sm_100a by oracle/build_ref.py) with its cupy host
+    glue restated on torch/cuFFT (oracle/refgpu.py), timed on this GPU at the
+    workload's size: R, RT and psi -> D -> |.|^2 of all projections."""
+    import torch
+    from oracle import refgpu
+    if not refgpu.available():
+        return {"unavailable": "oracle/_ref/libref_gpu.so not built (reference tree absent at build time)"}
+    from model_mosaic_b200.phantom import ellipsoid_volume_torch
+    torch.cuda.empty_cache()
+    dev = torch.device("cuda", local_rank)
+    n, nz, T = w["n"], w["nz"], w["ntheta"]
+    theta = np.linspace(0, w["theta_max"], T, endpoint=False).astype(np.float32)
+    inv_norm = float(np.float32(1.0 / np.sqrt(n / T)))
+    inv_beta = float(np.float32(1.0 / BETA_RATIO))
+    st = torch.cuda.current_stream()
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    obj = ellipsoid_volume_torch(n, nz, seed=0, device=dev)
+    tomo = refgpu.RefGpuTomoReal(n, nz, theta, device=dev)
+    sino = tomo.R(obj)
+    r_ms = timed(lambda: tomo.R(obj))
+    rt_ms = timed(lambda: tomo.RT(sino))
+    del tomo
+    torch.cuda.empty_cache()
+    prop = refgpu.RefGpuPropagation(n, nz, T, 1, 1.24e-9 / w["energy_kev"], w["voxelsize"], [w["distance"]],
+                                    device=dev)
+    d_ms = timed(lambda: refgpu.abs2(prop.D(refgpu.psi_from_proj(sino, inv_norm, inv_beta), 0)))
+    del prop, sino, obj
+    torch.cuda.empty_cache()
+    return {"R_ms": round(r_ms, 3), "RT_ms": round(rt_ms, 3), "D_ms": round(d_ms, 3),
+            "step_ms": round(r_ms + d_ms, 3),
+            "what": "the reference's kernels (processing/kernels.py) compiled for sm_100a with its host glue "
+                    "(processing/tomo.py, propagation.py, step3 psi/|.|^2) on torch/cuFFT, CUDA events, "
+                    "1 warm-up + 3 timed calls"}
+
+
 # ---------------------------------------------------------------- CPU (reference kernels on the host)
 def cpu_sample(w, slices=1, frames=32, cores=None):
     """Time the reference's kernels + restated glue on a bounded sample and
@@ -752,6 +830,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-rt", action="store_true", help="skip the adjoint (no scatter table)")
     ap.add_argument("--no-model", action="store_true", help="skip the fwd+grad timing of the model")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip the baseline legs that time the reference's own kernels on the GPU")
     ap.add_argument("--base", choices=sorted(WORKLOADS), default="production",
                     help="sizes for the fbp and paganin workloads (frames / sinogram of this workload)")
     ap.add_argument("--ups", type=int, default=2, help="stitch workload: mosaic of this upsampling factor")
@@ -806,6 +886,15 @@ def main():
         line = run_ours(args, w, rank, world, local_rank)
         if args.workload == "production" and not args.no_model:
             line["model_fwd_grad"] = run_model(args, local_rank)
+        if rank == 0 and world == 1 and args.workload == "production" and not args.no_ref_gpu:
+            ref = ref_gpu_ops(args, w, local_rank)
+            if "R_ms" in ref:
+                ops = line["ops"]
+                ref["speedup"] = {"R": round(ref["R_ms"] / ops["R_ms"], 3),
+                                  "RT": round(ref["RT_ms"] / ops["RT_ms"], 3) if ops["RT_ms"] else None,
+                                  "D": round(ref["D_ms"] / ops["D_ms"], 3),
+                                  "step": round(ref["step_ms"] / line["ms_per_step"], 3)}
+            line["reference_gpu"] = ref
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             t, desc, kind, cores = cpu_sample(w)
             V = w["nz"] * w["n"] ** 2

@@ -20,6 +20,7 @@
 //    by a radix sort of (cell, sample, tap) keys: deterministic, no atomics.
 #include "mm_common.cuh"
 #include "fft_smem.cuh"
+#include "tomo_kernels.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
@@ -42,6 +43,9 @@ struct mm_tomo {
     float2* d_twy = nullptr;     // Stockham twiddles of the 2n-point x and column transforms
     float2* d_twr = nullptr;     // Stockham twiddles of the n/2-point r transforms
     float2* d_exr = nullptr;     // e^{+2 pi i k/n}, k = 0..n/2 (real-from-half-length packing)
+    float2* col_scratch = nullptr;  // L2-resident per-SM regions of the 64 x 64 column transform
+    float2* col_tw = nullptr;       // its W_4096^(n2 k1) table
+    int sms = 0;
     bool fused_x = false, fused_r = false;
     // forward buffers
     float* P = nullptr;          // (zs, n, 2n)     padded phi*obj rows
@@ -1167,9 +1171,13 @@ int launch_col_fft_l(mm_tomo* h, const float2* src, float2* dst, cudaStream_t st
     return MM_OK;
 }
 
-// Column transform along v (length 2n) of the slice-interleaved spectrum.
+// Column transform along v (length 2n) of the slice-interleaved spectrum:
+// the 64 x 64 kernel with full-line accesses (tomo_col.cu) where it applies,
+// else one shared-memory block per four columns.
 template <bool INV>
 int launch_col_fft(mm_tomo* h, const float2* src, float2* dst, cudaStream_t st) {
+    const int rc = mmtomo::col_fft_pipe(h->n, h->zs, INV, src, dst, h->col_scratch, h->col_tw, h->sms, st);
+    if (rc != mmtomo::kNotCovered) return rc;
     switch (2 * h->n) {
         case 16: return launch_col_fft_l<16, INV>(h, src, dst, st);
         case 32: return launch_col_fft_l<32, INV>(h, src, dst, st);
@@ -1506,7 +1514,7 @@ void destroy(mm_tomo* h) {
     cufftHandle all[6] = {h->plan_xr2c, h->plan_xc2r, h->plan_y, h->plan_rc2r, h->plan_rr2c, h->plan_rc2c};
     for (cufftHandle p : all)
         if (p) cufftDestroy(p);
-    void* bufs[] = {h->d_cos, h->d_sin, h->d_phi1, h->d_twy, h->d_twr, h->d_exr, h->P, h->X, h->Y, h->F, h->Hh, h->sino_tmp, h->fft_work,
+    void* bufs[] = {h->d_cos, h->d_sin, h->d_phi1, h->d_twy, h->d_twr, h->d_exr, h->col_scratch, h->col_tw, h->P, h->X, h->Y, h->F, h->Hh, h->sino_tmp, h->fft_work,
                     h->csr_ptr, h->csr_idx, h->csr_w, h->chunk_task, h->chunk_pair, h->chunk_part, h->ypad, h->yc};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -1545,6 +1553,7 @@ extern "C" int mm_tomo_create(int n, int nz, int ntheta, const float* theta_host
     h->c1 = -3.141592653589793238f * 3.141592653589793238f / h->mu;
     h->phi_scale = (float)((double)(1 - n % 4) / (n * sqrt((double)n * ntheta)));
     cudaGetDevice(&h->device);
+    cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device);
 
     auto fail = [&](int rc) {
         destroy(h);
@@ -1603,6 +1612,18 @@ extern "C" int mm_tomo_create(int n, int nz, int ntheta, const float* theta_host
         if (mmfft::init_constants() != cudaSuccess) {
             mm::set_error("mm_tomo_create: FFT constant upload failed");
             return fail(MM_ECUDA);
+        }
+        size_t scr = 0, twn = 0;
+        if (mmtomo::col_fft_sizes(n, zs, h->sms, &scr, &twn) == MM_OK) {
+            std::vector<float2> twc(twn);
+            mmtomo::col_fft_twiddles(twc.data());
+            if ((rc = alloc(h, &h->col_scratch, scr, "column transform scratch")) ||
+                (rc = alloc(h, &h->col_tw, twn, "column transform twiddles")))
+                return fail(rc);
+            if (cudaMemcpy(h->col_tw, twc.data(), twn * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess) {
+                mm::set_error("mm_tomo_create: table upload failed");
+                return fail(MM_ECUDA);
+            }
         }
     }
     if (cudaMemcpy(h->d_cos, cs.data(), ntheta * 4, cudaMemcpyHostToDevice) != cudaSuccess ||

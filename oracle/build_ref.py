@@ -15,11 +15,19 @@ built here from its own source without cupy or a GPU.  This script
    ``threadIdx``/``blockIdx``/``blockDim`` built-ins as thread-local
    variables) and adds one launch driver per kernel that walks the grid;
 3. compiles it with ``g++ -fopenmp`` into ``oracle/_ref/libref_kernels.so``
-   and deletes the generated source.
+   and deletes the generated source;
+4. writes a second translation unit with the same kernel strings, verbatim,
+   behind ``#include <math.h>`` / ``#undef M_PI`` (the kernels declare their
+   own ``const float M_PI``) and one ``extern "C"`` launcher per kernel
+   (grid, block and stream as arguments), compiles it with nvcc for sm_100a
+   into ``oracle/_ref/libref_gpu.so`` and deletes the source.  That library
+   is the reference's GPU kernels as cupy would run them, for the GPU
+   reference harness (``oracle/refgpu.py``).
 
 Only ``oracle/_ref/`` is written; it is git-ignored (the reference source
 never enters the repository) but travels with the tree to the GPU box.
-Exit status 0 with a message when the reference tree is absent.
+Each library is rebuilt only when ``kernels.py`` is newer.  Exit status 0
+with a message when the reference tree is absent.
 """
 from __future__ import annotations
 
@@ -31,6 +39,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT_DIR, "libref_kernels.so")
+LIB_GPU = os.path.join(OUT_DIR, "libref_gpu.so")
 DEFAULT_REF = "/root/reference"
 
 SHIM = r"""
@@ -73,6 +82,25 @@ extern "C" void ref_launch_%(name)s(long gx, long gy, long gz %(params)s) {
 """
 
 
+GPU_PRELUDE = r"""
+#include <math.h>
+#include <cuda_runtime.h>
+#undef M_PI
+"""
+
+GPU_LAUNCHER = r"""
+extern "C" int refgpu_%(name)s(unsigned gx, unsigned gy, unsigned gz, unsigned bx, unsigned by, unsigned bz,
+                               void* stream %(params)s) {
+    %(name)s<<<dim3(gx, gy, gz), dim3(bx, by, bz), 0, (cudaStream_t)stream>>>(%(args)s);
+    return (int)cudaGetLastError();
+}
+"""
+
+
+def _fresh(lib: str, src: str) -> bool:
+    return os.path.exists(lib) and os.path.getmtime(lib) >= os.path.getmtime(src)
+
+
 def extract_kernels(kernels_py: str):
     """Return [(entry_name, source)] for every cp.RawKernel(src, name) call."""
     tree = ast.parse(open(kernels_py).read())
@@ -102,12 +130,47 @@ def _signature(src: str, name: str):
     return parts, names
 
 
-def build(ref_root: str = DEFAULT_REF, verbose: bool = True) -> str | None:
+def build_gpu(ref_root: str = DEFAULT_REF, verbose: bool = True, force: bool = False) -> str | None:
+    """The reference's kernel strings compiled for sm_100a with launchers."""
+    kp = os.path.join(ref_root, "processing", "kernels.py")
+    if not os.path.exists(kp):
+        return None
+    if not force and _fresh(LIB_GPU, kp):
+        return LIB_GPU
+    kernels = extract_kernels(kp)
+    os.makedirs(OUT_DIR, exist_ok=True)
+    tu = [GPU_PRELUDE]
+    for name, src in kernels:
+        tu.append(f"// ---- kernel source: processing/kernels.py entry '{name}' ----\n")
+        tu.append(src)
+    for name, src in kernels:
+        parts, names = _signature(src, name)
+        params = "".join(", " + p for p in parts)
+        tu.append(GPU_LAUNCHER % {"name": name, "params": params, "args": ", ".join(names)})
+    cu = os.path.join(OUT_DIR, "ref_kernels_gpu.cu")
+    with open(cu, "w") as f:
+        f.write("\n".join(tu))
+    nvcc = "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else "nvcc"
+    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-Xcompiler", "-fPIC", "-shared", "-w",
+           cu, "-o", LIB_GPU]
+    try:
+        subprocess.run(cmd, check=True)
+    finally:
+        os.remove(cu)
+    if verbose:
+        print(f"build_ref: {len(kernels)} kernels for sm_100a -> {LIB_GPU}")
+    return LIB_GPU
+
+
+def build(ref_root: str = DEFAULT_REF, verbose: bool = True, force: bool = False) -> str | None:
     kp = os.path.join(ref_root, "processing", "kernels.py")
     if not os.path.exists(kp):
         if verbose:
             print(f"build_ref: {kp} not found; oracle/_ref not rebuilt")
         return None
+    build_gpu(ref_root, verbose, force)
+    if not force and _fresh(LIB, kp):
+        return LIB
     kernels = extract_kernels(kp)
     os.makedirs(OUT_DIR, exist_ok=True)
     tu = [SHIM]

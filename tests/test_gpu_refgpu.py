@@ -1,0 +1,93 @@
+"""GPU parity against the reference's own CUDA kernels on the same GPU.
+
+The reference's kernel strings (processing/kernels.py) are compiled verbatim
+for sm_100a by oracle/build_ref.py and driven by oracle/refgpu.py, which
+restates the reference's cupy host code with torch (cuFFT).  This is the
+"cupy reference" of the specification run on this box: the product's R, RT
+and D are compared with it at the benchmark's geometry (2048-wide slices,
+2058 angles on [0, 2 pi), 64-row detector frames), where the CPU oracle
+would take minutes, and the reference's plain composed gradient of the
+differentiable model is compared with the FP64 oracle and the fused one.
+Gate: relative L2 <= 1e-5 (float32 against float32: both sides round)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import refgpu
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not refgpu.available(), reason="oracle/_ref/libref_gpu.so not built")]
+RTOL = 1e-5
+
+
+def rl2(a, b):
+    return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+
+@pytest.mark.parametrize("n,nz,T,tmax", [(128, 16, 180, np.pi), (2048, 4, 2058, 2 * np.pi)])
+def test_R_RT_vs_reference_gpu_kernels(n, nz, T, tmax):
+    from model_mosaic_b200.processing.tomo import TomoReal
+    from model_mosaic_b200.phantom import ellipsoid_volume_torch
+    theta = np.linspace(0, tmax, T, endpoint=False).astype(np.float32)
+    x = ellipsoid_volume_torch(n, nz, seed=11)
+    ref = refgpu.RefGpuTomoReal(n, nz, theta)
+    ours = TomoReal(n, nz, theta)
+    s_ref, s = ref.R(x), ours.R(x)
+    er = rl2(s, s_ref)
+    rec_ref, rec = ref.RT(s_ref), ours.RT(s_ref)
+    et = rl2(rec, rec_ref)
+    print(f"n={n} {T} angles: R rel-L2 vs reference kernels {er:.2e}, RT {et:.2e}")
+    assert er < RTOL and et < RTOL
+
+
+def test_D_vs_reference_gpu_kernels():
+    from model_mosaic_b200.processing.propagation import Propagation
+    n, nz, T = 2048, 64, 16
+    wl, vox, dist = 4.133e-11, 0.69e-6, 0.12
+    gen = torch.Generator(device="cuda").manual_seed(12)
+    psi = torch.complex(torch.randn((T, nz, n), generator=gen, device="cuda"),
+                        torch.randn((T, nz, n), generator=gen, device="cuda"))
+    ref = refgpu.RefGpuPropagation(n, nz, T, 1, wl, vox, [dist]).D(psi, 0)
+    got = Propagation(n, nz, T, 1, wl, vox, [dist]).D(psi, 0)
+    err = rl2(got, ref)
+    print(f"D 64x2048 frames: rel-L2 vs reference kernels {err:.2e}")
+    assert err < RTOL
+
+
+def test_reference_DT_is_adjoint():
+    n, nz, T = 256, 32, 4
+    p = refgpu.RefGpuPropagation(n, nz, T, 1, 4.133e-11, 0.69e-6, [0.12])
+    gen = torch.Generator(device="cuda").manual_seed(13)
+    a = torch.complex(torch.randn((T, nz, n), generator=gen, device="cuda"),
+                      torch.randn((T, nz, n), generator=gen, device="cuda")).to(torch.complex128)
+    b = torch.complex(torch.randn((T, nz, n), generator=gen, device="cuda"),
+                      torch.randn((T, nz, n), generator=gen, device="cuda")).to(torch.complex128)
+    lhs = torch.vdot(p.D(a.to(torch.complex64), 0).to(torch.complex128).flatten(), b.flatten())
+    rhs = torch.vdot(a.flatten(), p.DT(b.to(torch.complex64), 0).to(torch.complex128).flatten())
+    assert abs(complex(lhs - rhs)) / abs(complex(lhs)) < 1e-5
+
+
+def test_composed_gradient_matches_fused_and_oracle():
+    from model_mosaic_b200.model import ForwardModel
+    from model_mosaic_b200.phantom import ellipsoid_volume
+    from oracle.model import ModelOracle
+    n = nz = 64
+    T = 90
+    wl, vox, dist = 4.133e-11, 0.69e-6, 0.12
+    theta = np.linspace(0, np.pi, T, endpoint=False).astype(np.float32)
+    delta = ellipsoid_volume(n, nz, seed=0, vmin=0.2, vmax=1.0)
+    delta2 = ellipsoid_volume(n, nz, seed=1, vmin=0.2, vmax=1.0)
+    s = float(np.float32(1.5 / np.abs(ModelOracle(n, nz, theta, wl, vox, dist, s=1.0).tomo.R(delta)).max()))
+    ora = ModelOracle(n, nz, theta, wl, vox, dist, s=s)
+    d = ora.forward(delta2)
+    gref = ora.grad(delta, d)
+    dd, dl = torch.from_numpy(d.astype(np.float32)).cuda(), torch.from_numpy(delta).cuda()
+    tomo, prop = refgpu.RefGpuTomoReal(n, nz, theta), refgpu.RefGpuPropagation(n, nz, T, 1, wl, vox, [dist])
+    loss_r, g_r = refgpu.ref_loss_and_grad(tomo, prop, dl, dd, s, 0.01, chunk=32)
+    m = ForwardModel(n, nz, theta, wl, vox, dist, inv_norm=s, angle_chunk=32)
+    loss_f, g_f = m.loss_and_grad(dl, dd)
+    e_ref = float(np.linalg.norm(g_r.cpu().numpy() - gref) / np.linalg.norm(gref))
+    e_fused = float(np.linalg.norm(g_f.cpu().numpy() - gref) / np.linalg.norm(gref))
+    print(f"model gradient vs FP64: reference composition {e_ref:.2e}, fused {e_fused:.2e}")
+    assert e_ref < 1e-4 and e_fused < 1e-5
+    assert abs(float(loss_r) - float(loss_f)) / float(loss_f) < 1e-5
