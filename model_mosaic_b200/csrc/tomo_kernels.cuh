@@ -6,7 +6,7 @@
 namespace mmtomo {
 
 // Length-2n transforms along v of the slice-interleaved spectrum, (n+1)*zs
-// columns wide (tomo_col.cu), for 2n = 4096 and zs a multiple of 16.
+// columns wide (tomo_col.cu), for 2n = 4096 and zs a multiple of 8.
 // Forward (inv = false): src = Y, only the centre rows [n/2, 3n/2) are read,
 // rows beyond radius n + 16 of the spectrum origin are not stored.  Inverse:
 // src = F, rows beyond that radius are read as zeros, only the centre rows are

@@ -26,8 +26,13 @@ def rl2(a, b):
 
 @pytest.mark.parametrize("n,nz,T,tmax", [(128, 16, 180, np.pi), (2048, 4, 2058, 2 * np.pi)])
 def test_R_RT_vs_reference_gpu_kernels(n, nz, T, tmax):
+    # The reference's RT accumulates float32 atomics into the full (2n)^2
+    # grid; at 2058 angles its own rounding is ~1e-5.  Both adjoints are
+    # measured against the FP64 oracle on one slice: ours must meet RTOL, and
+    # the two may differ by no more than the reference's own error allows.
     from model_mosaic_b200.processing.tomo import TomoReal
     from model_mosaic_b200.phantom import ellipsoid_volume_torch
+    from oracle.usfft import TomoRealOracle
     theta = np.linspace(0, tmax, T, endpoint=False).astype(np.float32)
     x = ellipsoid_volume_torch(n, nz, seed=11)
     ref = refgpu.RefGpuTomoReal(n, nz, theta)
@@ -36,8 +41,14 @@ def test_R_RT_vs_reference_gpu_kernels(n, nz, T, tmax):
     er = rl2(s, s_ref)
     rec_ref, rec = ref.RT(s_ref), ours.RT(s_ref)
     et = rl2(rec, rec_ref)
-    print(f"n={n} {T} angles: R rel-L2 vs reference kernels {er:.2e}, RT {et:.2e}")
-    assert er < RTOL and et < RTOL
+    z = nz // 2
+    exact = torch.from_numpy(TomoRealOracle(n, 1, theta).RT(s_ref[:, z:z + 1].double().cpu().numpy())[0])
+    e_ours = rl2(rec[z].double().cpu(), exact)
+    e_ref = rl2(rec_ref[z].double().cpu(), exact)
+    print(f"n={n} {T} angles: R rel-L2 vs reference kernels {er:.2e}; RT vs reference {et:.2e}, "
+          f"vs FP64: ours {e_ours:.2e}, reference {e_ref:.2e}")
+    assert er < RTOL and e_ours < RTOL
+    assert et < max(RTOL, 1.5 * e_ref)
 
 
 def test_D_vs_reference_gpu_kernels():
