@@ -862,7 +862,7 @@ void destroy(mm_tomo* h) {
     for (cufftHandle p : all)
         if (p) cufftDestroy(p);
     void* bufs[] = {h->d_cos, h->d_sin, h->d_phi1, h->d_twy, h->d_twr, h->d_exr, h->col_scratch, h->col_tw, h->P, h->X, h->Y, h->F, h->Hh, h->sino_tmp, h->fft_work,
-                    h->csr_ptr, h->csr_idx, h->csr_w, h->piece_idx, h->piece_w, h->wfirst, h->chunk_task, h->chunk_pair, h->chunk_part, h->ypad, h->yc};
+                    h->csr_ptr, h->csr_idx, h->csr_w, h->chunk_task, h->chunk_pair, h->chunk_part, h->ypad, h->yc};
     for (void* b : bufs)
         if (b) cudaFree(b);
     delete h;

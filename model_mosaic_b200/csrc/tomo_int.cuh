@@ -44,11 +44,7 @@ struct mm_tomo {
     // pairs whose lists exceed kChunk entries (the cells around the spectrum
     // origin collect thousands) are summed in kChunk-entry pieces by separate
     // warps and combined in piece order
-    unsigned* piece_idx = nullptr;  // the long lists' entries (same format as csr_idx / csr_w)
-    float2* piece_w = nullptr;
-    unsigned* wfirst = nullptr;   // first pair of each streaming warp's range (<= 32 pairs)
-    long nwarps_stream = 0;
-    uint2* chunk_task = nullptr;  // (first, end) entry of each piece in piece_idx / piece_w
+    uint2* chunk_task = nullptr;  // (first, end) entry of each piece
     uint4* chunk_pair = nullptr;  // (pair, first piece, end piece, 0) per long pair
     float2* chunk_part = nullptr; // (pieces, 2, zs) partial sums: left and right cell
     long nchunks = 0, nlong = 0;

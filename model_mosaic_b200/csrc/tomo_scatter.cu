@@ -27,8 +27,7 @@ __device__ __forceinline__ void acc_add(float& s, float& c, float w, float v) {
     }
 }
 
-constexpr unsigned kChunk = 256;        // longest list one lane group sums alone
-constexpr unsigned kWarpEntries = 512;  // table entries per streaming warp (k_scatter_stream)
+constexpr unsigned kChunk = 256;  // longest list one lane group sums alone
 
 // Sums of the table entries [e0, e1) of one cell pair, left cell in al
 // (compensation cl), right cell in ar (cr).
@@ -165,108 +164,6 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict
     pair_sums<ZV, LPS, KAHAN>(e0, e1, idx, wgt, Q, zs, ln.zoff, ln.lane, al, cl, ar, cr);
     if (pc.keepL) ZVec<ZV>::store(A + pc.cell * zs + ln.zoff, al);
     if (pc.keepR) ZVec<ZV>::store(A + (pc.cell + 1) * zs + ln.zoff, ar);
-}
-
-// Streaming form of k_scatter for lane groups of a whole warp (64-slice
-// groups): warp w takes the cell pairs [wfirst[w], wfirst[w+1]) (at most 32,
-// about kWarpEntries table entries; balanced at build time) and walks their
-// entries, which are contiguous in the table, 32 at a time: one coalesced
-// load of the next 32 entries is in flight while the current 32 are summed,
-// and DEPTH spectrum rows are loaded before their sums.  A pair's sums are
-// stored when the walk passes its last entry.  Per pair the entries are
-// added in table order with the same arithmetic as pair_sums, so the results
-// are bitwise those of k_scatter.  The long lists are not in this table (their
-// pairs have empty lists here and are written afterwards by
-// k_scatter_combine).
-template <bool KAHAN, int ZSC>
-__global__ void __launch_bounds__(kThreads) k_scatter_stream(const unsigned* __restrict__ wfirst, long nwarps,
-                                                             const unsigned* __restrict__ ptr,
-                                                             const unsigned* __restrict__ idx,
-                                                             const float2* __restrict__ wgt,
-                                                             const float2* __restrict__ Q, float2* __restrict__ A,
-                                                             int zs_rt, int n, int prune) {
-    constexpr int ZV = 2, DEPTH = 8;
-    const unsigned FULL = 0xffffffffu;
-    const int zs = ZSC > 0 ? ZSC : zs_rt;
-    const int lane = threadIdx.x & 31;
-    const int zgroups = zs / 64;
-    const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long wr = warp / zgroups;
-    if (wr >= nwarps) return;
-    const int zoff = (int)(warp % zgroups) * 64 + lane * ZV;
-    const long P0 = __ldg(wfirst + wr);
-    const int np = (int)(__ldg(wfirst + wr + 1) - P0);   // 1 .. 32 pairs
-    const unsigned pst = lane < np ? __ldg(ptr + P0 + lane) : 0u;   // first entry of pair P0 + lane
-    const unsigned pend = __ldg(ptr + P0 + np);                     // end of the last pair
-    float al[2 * ZV], cl[2 * ZV], ar[2 * ZV], cr[2 * ZV];
-#pragma unroll
-    for (int q = 0; q < 2 * ZV; ++q) al[q] = cl[q] = ar[q] = cr[q] = 0.f;
-    int cur = 0;
-    auto end_of = [&](int i) {
-        const unsigned e = __shfl_sync(FULL, pst, (i + 1) & 31);
-        return i + 1 < np ? e : pend;
-    };
-    unsigned cend = end_of(0);
-    auto flush = [&]() {  // store pair P0 + cur, start the next
-        const PairCells pc(P0 + cur, n, prune);
-        if (pc.keepL) ZVec<ZV>::store(A + pc.cell * zs + zoff, al);
-        if (pc.keepR) ZVec<ZV>::store(A + (pc.cell + 1) * zs + zoff, ar);
-#pragma unroll
-        for (int q = 0; q < 2 * ZV; ++q) al[q] = cl[q] = ar[q] = cr[q] = 0.f;
-        ++cur;
-        cend = end_of(cur);
-    };
-    auto add = [&](unsigned ii, float2 w, const float* v) {
-        const float sl = (ii >> 31) ? -w.x : w.x, sr = ((ii >> 30) & 1u) ? -w.y : w.y;
-#pragma unroll
-        for (int q = 0; q < 2 * ZV; q += 2) {
-            acc_add<KAHAN>(al[q], cl[q], w.x, v[q]);
-            acc_add<KAHAN>(al[q + 1], cl[q + 1], sl, v[q + 1]);
-            acc_add<KAHAN>(ar[q], cr[q], w.y, v[q]);
-            acc_add<KAHAN>(ar[q + 1], cr[q + 1], sr, v[q + 1]);
-        }
-    };
-    const unsigned e0 = __shfl_sync(FULL, pst, 0);
-    unsigned mi = 0;
-    float2 mw = make_float2(0.f, 0.f);
-    if (e0 + lane < pend) {
-        mi = __ldg(idx + e0 + lane);
-        mw = __ldg(wgt + e0 + lane);
-    }
-    for (unsigned base = e0; base < pend; base += 32) {
-        const int cnt = (int)min(32u, pend - base);
-        unsigned ni = 0;
-        float2 nw = make_float2(0.f, 0.f);
-        if (base + 32 + lane < pend) {
-            ni = __ldg(idx + base + 32 + lane);
-            nw = __ldg(wgt + base + 32 + lane);
-        }
-        for (int k = 0; k < cnt; k += DEPTH) {
-            unsigned ii[DEPTH];
-            float2 ww[DEPTH];
-            float vv[DEPTH][2 * ZV];
-#pragma unroll
-            for (int u = 0; u < DEPTH; ++u) {
-                ii[u] = __shfl_sync(FULL, mi, k + u);
-                ww[u].x = __shfl_sync(FULL, mw.x, k + u);
-                ww[u].y = __shfl_sync(FULL, mw.y, k + u);
-            }
-#pragma unroll
-            for (int u = 0; u < DEPTH; ++u)
-                if (k + u < cnt) ZVec<ZV>::load(Q + (long)(ii[u] & 0x3fffffffu) * zs + zoff, vv[u]);
-#pragma unroll
-            for (int u = 0; u < DEPTH; ++u) {
-                if (k + u < cnt) {
-                    const unsigned ent = base + k + u;
-                    while (ent >= cend) flush();
-                    add(ii[u], ww[u], vv[u]);
-                }
-            }
-        }
-        mi = ni;
-        mw = nw;
-    }
-    while (cur < np) flush();
 }
 
 // Pieces of the long lists: partial sums of kChunk entries each.  With
@@ -448,19 +345,11 @@ int launch_scatter_t(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) {
     if (h->nchunks > 0) {  // the long lists' pieces first: they are the longest chains
         auto kp = kh ? (z64 ? k_scatter_pieces<ZV, LPS, true, Z64> : k_scatter_pieces<ZV, LPS, true, 0>)
                      : (z64 ? k_scatter_pieces<ZV, LPS, false, Z64> : k_scatter_pieces<ZV, LPS, false, 0>);
-        kp<<<grid(h->nchunks), kThreads, 0, st>>>(h->chunk_task, h->piece_idx, h->piece_w, Q, h->chunk_part,
+        kp<<<grid(h->nchunks), kThreads, 0, st>>>(h->chunk_task, h->csr_idx, h->csr_w, Q, h->chunk_part,
                                                   h->nchunks, h->zs);
         MM_LAUNCHED();
     }
-    if (LPS == 32 && h->wfirst) {  // whole-warp lane groups: the streaming walk over balanced pair ranges
-        auto ks = kh ? (z64 ? k_scatter_stream<true, 64> : k_scatter_stream<true, 0>)
-                     : (z64 ? k_scatter_stream<false, 64> : k_scatter_stream<false, 0>);
-        const long w = h->nwarps_stream * (h->zs / 64);
-        ks<<<(unsigned)((w * 32 + kThreads - 1) / kThreads), kThreads, 0, st>>>(
-            h->wfirst, h->nwarps_stream, h->csr_ptr, h->csr_idx, h->csr_w, Q, A, h->zs, h->n, prune);
-    } else {
-        kern<<<blocks, kThreads, 0, st>>>(h->csr_ptr, h->csr_idx, h->csr_w, Q, A, npairs, h->zs, h->n, prune);
-    }
+    kern<<<blocks, kThreads, 0, st>>>(h->csr_ptr, h->csr_idx, h->csr_w, Q, A, npairs, h->zs, h->n, prune);
     MM_LAUNCHED();
     if (h->nlong > 0) {
         auto kc = kh ? (z64 ? k_scatter_combine<ZV, LPS, true, Z64> : k_scatter_combine<ZV, LPS, true, 0>)
@@ -562,93 +451,24 @@ int build_csr(mm_tomo* h, cudaStream_t st) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail_cuda(e);
     cleanup();
-    // long lists -> pieces of kChunk entries (fixed split: deterministic), in
-    // a table of their own; the main table keeps every other list (the long
-    // pairs get empty lists there)
+    // long lists -> pieces of kChunk entries (fixed split: deterministic)
     std::vector<unsigned> hp(npairs + 1);
     MM_CUDA(cudaMemcpy(hp.data(), h->csr_ptr, hp.size() * sizeof(unsigned), cudaMemcpyDeviceToHost));
     std::vector<uint2> tasks;
     std::vector<uint4> longp;
-    size_t npiece = 0;
     for (long q = 0; q < npairs; ++q) {
         const unsigned a = hp[q], b = hp[q + 1];
         if (b - a <= kChunk) continue;
         const unsigned t0 = (unsigned)tasks.size();
-        for (unsigned x = a; x < b; x += kChunk)
-            tasks.push_back(make_uint2((unsigned)(npiece + (x - a)), (unsigned)(npiece + std::min(b, x + kChunk) - a)));
+        for (unsigned x = a; x < b; x += kChunk) tasks.push_back(make_uint2(x, std::min(b, x + kChunk)));
         longp.push_back(make_uint4((unsigned)q, t0, (unsigned)tasks.size(), 0u));
-        npiece += b - a;
     }
     if (!longp.empty()) {
         MM_TRY(alloc(h, &h->chunk_task, tasks.size(), "scatter pieces"));
         MM_TRY(alloc(h, &h->chunk_pair, longp.size(), "scatter long pairs"));
         MM_TRY(alloc(h, &h->chunk_part, tasks.size() * 2 * (size_t)h->zs, "scatter partial sums"));
-        MM_TRY(alloc(h, &h->piece_idx, npiece, "scatter piece entries"));
-        MM_TRY(alloc(h, &h->piece_w, npiece, "scatter piece weights"));
         MM_CUDA(cudaMemcpy(h->chunk_task, tasks.data(), tasks.size() * sizeof(uint2), cudaMemcpyHostToDevice));
         MM_CUDA(cudaMemcpy(h->chunk_pair, longp.data(), longp.size() * sizeof(uint4), cudaMemcpyHostToDevice));
-        // move the long lists' entries out and close the gaps in the main table
-        const size_t nmain = (size_t)nnz - npiece;
-        unsigned* nidx = nullptr;
-        float2* nw = nullptr;
-        MM_TRY(alloc(h, &nidx, std::max<size_t>(nmain, 1), "scatter sample index"));
-        MM_TRY(alloc(h, &nw, std::max<size_t>(nmain, 1), "scatter weights"));
-        size_t poff = 0, from = 0, to = 0;
-        auto run = [&](size_t a, size_t b) -> int {  // main-table entries [a, b) of the old table
-            if (b > a) {
-                MM_CUDA(cudaMemcpyAsync(nidx + to, h->csr_idx + a, (b - a) * sizeof(unsigned), cudaMemcpyDeviceToDevice, st));
-                MM_CUDA(cudaMemcpyAsync(nw + to, h->csr_w + a, (b - a) * sizeof(float2), cudaMemcpyDeviceToDevice, st));
-                to += b - a;
-            }
-            return MM_OK;
-        };
-        for (const uint4& lp : longp) {
-            const size_t a = hp[lp.x], b = hp[lp.x + 1];
-            MM_TRY(run(from, a));
-            MM_CUDA(cudaMemcpyAsync(h->piece_idx + poff, h->csr_idx + a, (b - a) * sizeof(unsigned),
-                                    cudaMemcpyDeviceToDevice, st));
-            MM_CUDA(cudaMemcpyAsync(h->piece_w + poff, h->csr_w + a, (b - a) * sizeof(float2), cudaMemcpyDeviceToDevice,
-                                    st));
-            poff += b - a;
-            from = b;
-        }
-        MM_TRY(run(from, (size_t)nnz));
-        std::vector<unsigned> hp2(npairs + 1);
-        size_t shift = 0, li = 0;
-        for (long q = 0; q <= npairs; ++q) {
-            hp2[q] = (unsigned)(hp[q] - shift);
-            if (li < longp.size() && (long)longp[li].x == q) {
-                shift += hp[q + 1] - hp[q];
-                ++li;
-            }
-        }
-        MM_CUDA(cudaMemcpyAsync(h->csr_ptr, hp2.data(), hp2.size() * sizeof(unsigned), cudaMemcpyHostToDevice, st));
-        MM_CUDA(cudaStreamSynchronize(st));
-        cudaFree(h->csr_idx);
-        cudaFree(h->csr_w);
-        h->ws_bytes -= (size_t)nnz * (sizeof(unsigned) + sizeof(float2));
-        h->csr_idx = nidx;
-        h->csr_w = nw;
-        hp.swap(hp2);
-    }
-    // balanced ranges of at most 32 pairs for the streaming scatter
-    {
-        std::vector<unsigned> wf(1, 0u);
-        unsigned cnt = 0, ent = 0;
-        for (long q = 0; q < npairs; ++q) {
-            const unsigned len = hp[q + 1] - hp[q];
-            if (cnt == 32 || (cnt > 0 && ent + len > kWarpEntries)) {
-                wf.push_back((unsigned)q);
-                cnt = 0;
-                ent = 0;
-            }
-            ++cnt;
-            ent += len;
-        }
-        wf.push_back((unsigned)npairs);
-        MM_TRY(alloc(h, &h->wfirst, wf.size(), "scatter warp ranges"));
-        MM_CUDA(cudaMemcpy(h->wfirst, wf.data(), wf.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
-        h->nwarps_stream = (long)wf.size() - 1;
     }
     h->nchunks = (long)tasks.size();
     h->nlong = (long)longp.size();
