@@ -38,14 +38,21 @@ typedef struct mm_fbp mm_fbp;
 typedef struct mm_pgn mm_pgn;
 
 /* USFFT options.  Zero-initialised fields take the reference defaults
- * (processing/tomo.py:39-42): eps = 1e-3, m from eps (m = 4), oversampling 2. */
+ * (processing/tomo.py:39-42): eps = 1e-3, m from eps (m = 4), oversampling 2.
+ * The adjoint's scatter table is built per block of angles, sized by the
+ * free device memory; blocks after the first add into the first block's
+ * result.  When all blocks do not fit at once (very large n and angle
+ * counts, e.g. n = 24576 with 18432 angles) they are rebuilt one at a time
+ * at every RT call. */
 typedef struct mm_tomo_opts {
     double eps;        /* Gaussian accuracy; <= 0 -> 1e-3 */
     int    m;          /* half-width override; <= 0 -> from eps (reference formula) */
     int    clamp_xy;   /* 1: clamp sample coordinates to [-1/2, 1/2 - 1e-5] in R as
                           TomoLargeReal's gather does (processing/kernels.py:478-481) */
     int    compensated;  /* 1: Kahan-compensated sums in the adjoint scatter */
-    int    reserved[4];
+    int    max_table_angles;  /* > 0: at most this many angles per block of the adjoint's
+                                 scatter table (0: as many as device memory allows) */
+    int    reserved[3];
 } mm_tomo_opts;
 
 /* Library and error reporting. */
@@ -56,7 +63,7 @@ int         mm_last_error(char* buf, size_t len);  /* copies the message, return
  * mm_tomo_create replaces TomoReal.__init__(n, nz, theta)
  *   (processing/tomo.py:30-88) and TomoLargeReal.__init__(n, theta, chunk_xy)
  *   (processing/tomo_large.py:72-148).  theta_host: ntheta float32 radians.
- *   opts may be NULL (reference defaults).  n must be even, 8 <= n <= 16384. */
+ *   opts may be NULL (reference defaults).  n must be even, 8 <= n <= 32768. */
 int mm_tomo_create(int n, int nz, int ntheta, const float* theta_host,
                    const mm_tomo_opts* opts, mm_tomo** out);
 /* Replaces TomoReal.free (processing/tomo.py:109-119) / TomoLargeReal.free. */
@@ -102,7 +109,7 @@ int mm_tomo_get_timing(mm_tomo* h, double* ms, long long* calls, int nstages, lo
  * mm_prop_create replaces Propagation.__init__(n, nz, ntheta, ndist,
  *   wavelength, voxelsize, distance) (processing/propagation.py:18-35) and
  *   PropagationLarge.__init__ (processing/propagation_large.py:55-94).
- *   Any n, nz in [2, 16384]: powers of two up to 2048 run the fused
+ *   Any n, nz in [2, 32768]: powers of two up to 2048 run the fused
  *   two-pass kernels, other sizes the general path (cuFFT 2-D transforms
  *   between reordering kernels). */
 int mm_prop_create(int n, int nz, int ntheta, int ndist, double wavelength,

@@ -359,8 +359,18 @@ int gen_plan(mm_prop* h, int nt, cufftHandle* out) {
         h->plan_part = 0;
     }
     if (!*slot) {
-        int dims[2] = {h->nz, h->n};
-        MM_CUFFT(cufftPlanMany(slot, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, nt));
+        // 64-bit plan: a batch of frames of the largest sizes (24576^2 and up)
+        // holds more than 2^31 elements
+        long long dims[2] = {h->nz, h->n};
+        size_t ws = 0;
+        MM_CUFFT(cufftCreate(slot));
+        const cufftResult r = cufftMakePlanMany64(*slot, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, nt, &ws);
+        if (r != CUFFT_SUCCESS) {
+            cufftDestroy(*slot);
+            *slot = 0;
+            mm::set_error("cufftMakePlanMany64 (%d frames of %d x %d): %s", nt, h->nz, h->n, mm::cufft_name(r));
+            return MM_ECUFFT;
+        }
         if (nt != h->ntheta) h->part_batch = nt;
     }
     *out = *slot;
@@ -455,7 +465,7 @@ extern "C" int mm_prop_create(int n, int nz, int ntheta, int ndist, double wavel
                               const double* distance_host, mm_prop** out) {
     MM_REQUIRE(out != nullptr, "mm_prop_create: out is NULL");
     *out = nullptr;
-    MM_REQUIRE(n >= 2 && n <= 16384 && nz >= 2 && nz <= 16384, "mm_prop_create: n=%d, nz=%d outside [2, 16384]", n,
+    MM_REQUIRE(n >= 2 && n <= 32768 && nz >= 2 && nz <= 32768, "mm_prop_create: n=%d, nz=%d outside [2, 32768]", n,
                nz);
     MM_REQUIRE(ntheta >= 1 && ndist >= 1 && distance_host != nullptr, "mm_prop_create: bad ntheta/ndist");
     MM_REQUIRE(voxelsize > 0, "mm_prop_create: voxelsize must be positive");

@@ -858,11 +858,12 @@ int ensure_rt(mm_tomo* h, cudaStream_t st) {
 
 void destroy(mm_tomo* h) {
     h->tm.release();
+    mmtomo::free_tables(h);
     cufftHandle all[6] = {h->plan_xr2c, h->plan_xc2r, h->plan_y, h->plan_rc2r, h->plan_rr2c, h->plan_rc2c};
     for (cufftHandle p : all)
         if (p) cufftDestroy(p);
     void* bufs[] = {h->d_cos, h->d_sin, h->d_phi1, h->d_twy, h->d_twr, h->d_exr, h->col_scratch, h->col_tw, h->P, h->X, h->Y, h->F, h->Hh, h->sino_tmp, h->fft_work,
-                    h->csr_ptr, h->csr_idx, h->csr_w, h->chunk_task, h->chunk_pair, h->chunk_part, h->ypad, h->yc};
+                    h->ypad, h->yc};
     for (void* b : bufs)
         if (b) cudaFree(b);
     delete h;
@@ -875,13 +876,14 @@ extern "C" int mm_tomo_create(int n, int nz, int ntheta, const float* theta_host
                               mm_tomo** out) {
     MM_REQUIRE(out != nullptr, "mm_tomo_create: out is NULL");
     *out = nullptr;
-    MM_REQUIRE(n >= 8 && n <= 16384 && n % 2 == 0, "mm_tomo_create: n=%d must be even and in [8, 16384]", n);
+    MM_REQUIRE(n >= 8 && n <= 32768 && n % 2 == 0, "mm_tomo_create: n=%d must be even and in [8, 32768]", n);
     MM_REQUIRE(nz >= 1 && nz <= 4096, "mm_tomo_create: nz=%d out of range", nz);
     MM_REQUIRE(ntheta >= 1 && theta_host != nullptr, "mm_tomo_create: need ntheta >= 1 angles");
     const double eps = (opts && opts->eps > 0) ? opts->eps : 1e-3;
     const double mu = -log(eps) / (2.0 * n * n);
     int m = (int)ceil(2.0 * n / M_PI * sqrt(-mu * log(eps) + (mu * n) * (mu * n) / 4.0));
     if (opts && opts->m > 0) m = opts->m;
+    MM_REQUIRE(!opts || opts->max_table_angles >= 0, "mm_tomo_create: max_table_angles must be >= 0");
     MM_REQUIRE(m >= 2 && m <= 6, "mm_tomo_create: m=%d unsupported (2..6)", m);
 
     mm_tomo* h = new mm_tomo();
@@ -892,6 +894,7 @@ extern "C" int mm_tomo_create(int n, int nz, int ntheta, const float* theta_host
     h->K = n / 2 + 1;
     h->clamp = (opts && opts->clamp_xy) ? 1 : 0;
     h->compensated = (opts && opts->compensated) ? 1 : 0;
+    h->table_angles = opts ? opts->max_table_angles : 0;
     int zs = 1;
     while (zs < nz) zs <<= 1;
     h->zs = zs;
@@ -1108,7 +1111,7 @@ int rt_tail(mm_tomo* h, cudaStream_t st) {
     const int n = h->n, zs = h->zs;
     h->tm.begin(7, st);
     MM_TRY(mmtomo::launch_scatter(h, h->Hh, h->F, st));
-    h->tm.end(st, 1 + (h->nchunks > 0) + (h->nlong > 0));
+    h->tm.end(st, 0);
     h->tm.begin(8, st);
     int rc = launch_col_fft<true>(h, h->F, h->Y, st);
     if (rc == -100) {

@@ -8,6 +8,25 @@
 #include <cuda_bf16.h>
 #include <cufft.h>
 
+#include <vector>
+
+// The adjoint's static scatter table for the angles [t0, t1): destination
+// cell pair (row, 2p), (row, 2p+1) -> entries (sample, conj bits) + weights.
+struct ScatterTable {
+    int t0 = 0, t1 = 0;
+    unsigned* ptr = nullptr;      // npairs + 1
+    unsigned* idx = nullptr;      // sample index (k*T + t) | conj left << 31 | conj right << 30
+    float2* w = nullptr;          // (left, right) weights
+    // pairs whose lists exceed kChunk entries (the cells around the spectrum
+    // origin collect thousands) are summed in kChunk-entry pieces by separate
+    // warps and combined in piece order
+    uint2* chunk_task = nullptr;  // (first, end) entry of each piece
+    uint4* chunk_pair = nullptr;  // (pair, first piece, end piece, 0) per long pair
+    float2* chunk_part = nullptr; // (pieces, 2, zs) partial sums: left and right cell
+    long nchunks = 0, nlong = 0, nnz = 0;
+    size_t bytes = 0;
+};
+
 struct mm_tomo {
     int n = 0, nz = 0, ntheta = 0, m = 0, zs = 0, K = 0, clamp = 0, compensated = 0;
     int paired = 0;  // angles symmetric under theta -> theta + pi: the gather takes them in pairs
@@ -36,18 +55,12 @@ struct mm_tomo {
     bool plans_rt = false, plans_c = false;
     bool y_dirty = false;        // RT used Y as scratch: its zero pad rows need restoring
     // adjoint scatter table
+    // adjoint scatter tables, one per block of angles (the scatter of every
+    // block after the first adds into the first one's result)
     bool csr_ready = false;
-    unsigned* csr_ptr = nullptr;  // npairs + 1 (cell pairs (row, 2p), (row, 2p+1))
-    unsigned* csr_idx = nullptr;  // sample index (k*T + t) | conj left << 31 | conj right << 30
-    float2* csr_w = nullptr;      // (left, right) weights
-    size_t nnz = 0;
-    // pairs whose lists exceed kChunk entries (the cells around the spectrum
-    // origin collect thousands) are summed in kChunk-entry pieces by separate
-    // warps and combined in piece order
-    uint2* chunk_task = nullptr;  // (first, end) entry of each piece
-    uint4* chunk_pair = nullptr;  // (pair, first piece, end piece, 0) per long pair
-    float2* chunk_part = nullptr; // (pieces, 2, zs) partial sums: left and right cell
-    long nchunks = 0, nlong = 0;
+    bool tables_resident = true;  // false: rebuilt block by block at every RT call
+    int table_angles = 0;         // angles per table block
+    std::vector<ScatterTable> tabs;
     float* ypad = nullptr;       // (T, zs, n) real sino padded in z (nz < zs)
     float2* yc = nullptr;        // (T, zs, n) complex sino spectrum (complex RT)
     size_t ws_bytes = 0;
@@ -205,5 +218,6 @@ int pick_lanes(int zs, int& ZV, int& LPS) {
 namespace mmtomo {
 // tomo_scatter.cu
 int build_csr(mm_tomo* h, cudaStream_t st);
+void free_tables(mm_tomo* h);
 int launch_scatter(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st);
 }  // namespace mmtomo

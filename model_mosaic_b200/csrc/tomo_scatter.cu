@@ -137,6 +137,33 @@ struct ScatterLanes {
     }
 };
 
+// Store (acc = 0) or add (acc != 0: a later block of angles) the sums of a
+// cell pair.  Each cell belongs to exactly one lane group per launch.
+template <int ZV>
+__device__ __forceinline__ void store_cells(float2* __restrict__ A, const PairCells& pc, int zs, int zoff, float* al,
+                                            float* ar, int acc) {
+    if (pc.keepL) {
+        float2* d = A + pc.cell * zs + zoff;
+        if (acc) {
+            float o[2 * ZV];
+            ZVec<ZV>::load(d, o);
+#pragma unroll
+            for (int q = 0; q < 2 * ZV; ++q) al[q] += o[q];
+        }
+        ZVec<ZV>::store(d, al);
+    }
+    if (pc.keepR) {
+        float2* d = A + (pc.cell + 1) * zs + zoff;
+        if (acc) {
+            float o[2 * ZV];
+            ZVec<ZV>::load(d, o);
+#pragma unroll
+            for (int q = 0; q < 2 * ZV; ++q) ar[q] += o[q];
+        }
+        ZVec<ZV>::store(d, ar);
+    }
+}
+
 // RT: pull-scatter over the static pair table.  One lane group per pair of
 // horizontally adjacent cells (row, 2p) and (row, 2p+1): the two cells
 // receive almost the same samples (8 of a window's 9 columns cover both), so
@@ -149,7 +176,7 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict
                                                       const unsigned* __restrict__ idx,
                                                       const float2* __restrict__ wgt,
                                                       const float2* __restrict__ Q, float2* __restrict__ A,
-                                                      long npairs, int zs_rt, int n, int prune) {
+                                                      long npairs, int zs_rt, int n, int prune, int acc) {
     const int zs = ZSC > 0 ? ZSC : zs_rt;  // compile-time slice count: immediate offsets
     const ScatterLanes<ZV, LPS> ln(zs);
     const long p = ln.item;
@@ -158,12 +185,12 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const unsigned* __restrict
     if (!pc.keepL && !pc.keepR) return;
     const unsigned e0 = __ldg(ptr + p), e1 = __ldg(ptr + p + 1);
     if (e1 - e0 > kChunk) return;
+    if (acc && e1 == e0) return;
     float al[2 * ZV], cl[2 * ZV], ar[2 * ZV], cr[2 * ZV];
 #pragma unroll
     for (int q = 0; q < 2 * ZV; ++q) al[q] = cl[q] = ar[q] = cr[q] = 0.f;
     pair_sums<ZV, LPS, KAHAN>(e0, e1, idx, wgt, Q, zs, ln.zoff, ln.lane, al, cl, ar, cr);
-    if (pc.keepL) ZVec<ZV>::store(A + pc.cell * zs + ln.zoff, al);
-    if (pc.keepR) ZVec<ZV>::store(A + (pc.cell + 1) * zs + ln.zoff, ar);
+    store_cells<ZV>(A, pc, zs, ln.zoff, al, ar, acc);
 }
 
 // Pieces of the long lists: partial sums of kChunk entries each.  With
@@ -198,7 +225,7 @@ template <int ZV, int LPS, bool KAHAN, int ZSC>
 __global__ void __launch_bounds__(kThreads) k_scatter_combine(const uint4* __restrict__ lp,
                                                               const float2* __restrict__ part,
                                                               float2* __restrict__ A, long nlong, int zs_rt, int n,
-                                                              int prune) {
+                                                              int prune, int acc) {
     const int zs = ZSC > 0 ? ZSC : zs_rt;
     const ScatterLanes<ZV, LPS> ln(zs);
     if (ln.item >= nlong) return;
@@ -218,8 +245,7 @@ __global__ void __launch_bounds__(kThreads) k_scatter_combine(const uint4* __res
             acc_add<KAHAN>(ar[q], cr[q], 1.0f, vr[q]);
         }
     }
-    if (pc.keepL) ZVec<ZV>::store(A + pc.cell * zs + ln.zoff, al);
-    if (pc.keepR) ZVec<ZV>::store(A + (pc.cell + 1) * zs + ln.zoff, ar);
+    store_cells<ZV>(A, pc, zs, ln.zoff, al, ar, acc);
 }
 
 // Scatter-table construction ---------------------------------------------
@@ -244,15 +270,17 @@ __device__ __forceinline__ void tap_dest(long e, int n, int T, const float* __re
     tap_cell(g.bx + i0, g.by + i1, n, row, col, cj);
 }
 
+// A table block covers the taps e0 .. e0 + nent - 1 (whole angles); keys
+// carry the tap's offset e - e0 within the block.
 template <int M>
 __global__ void k_pair_keys(unsigned long long* __restrict__ keys, const float* __restrict__ cosT,
-                            const float* __restrict__ sinT, int n, int T, long nent) {
+                            const float* __restrict__ sinT, int n, int T, long nent, long e0) {
     const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nent) return;
     SampleGeo g;
     int k, t, i0, i1, row, col;
     bool cj;
-    tap_dest<M>(e, n, T, cosT, sinT, g, k, t, i0, i1, row, col, cj);
+    tap_dest<M>(e0 + e, n, T, cosT, sinT, g, k, t, i0, i1, row, col, cj);
     const unsigned long long pair = (unsigned long long)row * (n / 2 + 1) + (col >> 1);
     keys[e] = (pair << 33) | ((unsigned long long)e << 1) | (unsigned long long)(col & 1);
 }
@@ -293,7 +321,7 @@ __global__ void k_pair_payload(const unsigned long long* __restrict__ keys, cons
                                const unsigned* __restrict__ pos, unsigned* __restrict__ idx,
                                float2* __restrict__ wgt, unsigned* __restrict__ pairs,
                                const float* __restrict__ cosT, const float* __restrict__ sinT, int n, int T,
-                               long nent, float c0, float c1, float scale) {
+                               long nent, long e0, float c0, float c1, float scale) {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nent || !head[i]) return;
     const bool merged = i + 1 < nent && !head[i + 1];
@@ -304,7 +332,7 @@ __global__ void k_pair_payload(const unsigned long long* __restrict__ keys, cons
         SampleGeo g;
         int k, t, i0, i1, row, col;
         bool cj;
-        tap_dest<M>((long)((key >> 1) & 0xffffffffull), n, T, cosT, sinT, g, k, t, i0, i1, row, col, cj);
+        tap_dest<M>(e0 + (long)((key >> 1) & 0xffffffffull), n, T, cosT, sinT, g, k, t, i0, i1, row, col, cj);
         const int half = (int)(key & 1);
         w[half] = tap_wgt<M>(g, k, i0, i1, n, c0, c1, scale);
         if (cj != g.mir) conj |= half ? 0x40000000u : 0x80000000u;
@@ -326,7 +354,7 @@ __global__ void k_pair_ptr(const unsigned* __restrict__ pairs, unsigned* __restr
 }
 
 template <int ZV, int LPS>
-int launch_scatter_t(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) {
+int launch_scatter_t(mm_tomo* h, const ScatterTable& tb, const float2* Q, float2* A, int acc, cudaStream_t st) {
     const long npairs = 2L * h->n * (h->n / 2 + 1);
     const long warps = ((npairs + (32 / LPS) - 1) / (32 / LPS)) * (h->zs / (LPS * ZV));
     const long blocks = (warps * 32 + kThreads - 1) / kThreads;
@@ -342,43 +370,66 @@ int launch_scatter_t(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) {
         const long w = ((items + (32 / LPS) - 1) / (32 / LPS)) * (h->zs / (LPS * ZV));
         return (unsigned)((w * 32 + kThreads - 1) / kThreads);
     };
-    if (h->nchunks > 0) {  // the long lists' pieces first: they are the longest chains
+    if (tb.nchunks > 0) {  // the long lists' pieces first: they are the longest chains
         auto kp = kh ? (z64 ? k_scatter_pieces<ZV, LPS, true, Z64> : k_scatter_pieces<ZV, LPS, true, 0>)
                      : (z64 ? k_scatter_pieces<ZV, LPS, false, Z64> : k_scatter_pieces<ZV, LPS, false, 0>);
-        kp<<<grid(h->nchunks), kThreads, 0, st>>>(h->chunk_task, h->csr_idx, h->csr_w, Q, h->chunk_part,
-                                                  h->nchunks, h->zs);
+        kp<<<grid(tb.nchunks), kThreads, 0, st>>>(tb.chunk_task, tb.idx, tb.w, Q, tb.chunk_part, tb.nchunks, h->zs);
         MM_LAUNCHED();
     }
-    kern<<<blocks, kThreads, 0, st>>>(h->csr_ptr, h->csr_idx, h->csr_w, Q, A, npairs, h->zs, h->n, prune);
+    kern<<<blocks, kThreads, 0, st>>>(tb.ptr, tb.idx, tb.w, Q, A, npairs, h->zs, h->n, prune, acc);
     MM_LAUNCHED();
-    if (h->nlong > 0) {
+    if (tb.nlong > 0) {
         auto kc = kh ? (z64 ? k_scatter_combine<ZV, LPS, true, Z64> : k_scatter_combine<ZV, LPS, true, 0>)
                      : (z64 ? k_scatter_combine<ZV, LPS, false, Z64> : k_scatter_combine<ZV, LPS, false, 0>);
-        kc<<<grid(h->nlong), kThreads, 0, st>>>(h->chunk_pair, h->chunk_part, A, h->nlong, h->zs, h->n, prune);
+        kc<<<grid(tb.nlong), kThreads, 0, st>>>(tb.chunk_pair, tb.chunk_part, A, tb.nlong, h->zs, h->n, prune, acc);
         MM_LAUNCHED();
     }
     return MM_OK;
 }
 
-int launch_scatter(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) {
+int launch_table(mm_tomo* h, const ScatterTable& tb, const float2* Q, float2* A, int acc, cudaStream_t st) {
     int ZV, LPS;
     pick_lanes(h->zs, ZV, LPS);
-    if (ZV == 1) return launch_scatter_t<1, 1>(h, Q, A, st);
+    if (ZV == 1) return launch_scatter_t<1, 1>(h, tb, Q, A, acc, st);
     switch (LPS) {
-        case 1: return launch_scatter_t<2, 1>(h, Q, A, st);
-        case 2: return launch_scatter_t<2, 2>(h, Q, A, st);
-        case 4: return launch_scatter_t<2, 4>(h, Q, A, st);
-        case 8: return launch_scatter_t<2, 8>(h, Q, A, st);
-        case 16: return launch_scatter_t<2, 16>(h, Q, A, st);
-        default: return launch_scatter_t<2, 32>(h, Q, A, st);
+        case 1: return launch_scatter_t<2, 1>(h, tb, Q, A, acc, st);
+        case 2: return launch_scatter_t<2, 2>(h, tb, Q, A, acc, st);
+        case 4: return launch_scatter_t<2, 4>(h, tb, Q, A, acc, st);
+        case 8: return launch_scatter_t<2, 8>(h, tb, Q, A, acc, st);
+        case 16: return launch_scatter_t<2, 16>(h, tb, Q, A, acc, st);
+        default: return launch_scatter_t<2, 32>(h, tb, Q, A, acc, st);
     }
 }
 
-int build_csr(mm_tomo* h, cudaStream_t st) {
-    if (h->csr_ready) return MM_OK;
-    h->tm.begin(12, st);
+void free_table(mm_tomo* h, ScatterTable& tb) {
+    void* bufs[] = {tb.ptr, tb.idx, tb.w, tb.chunk_task, tb.chunk_pair, tb.chunk_part};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    h->ws_bytes -= tb.bytes;
+    const int t0 = tb.t0, t1 = tb.t1;
+    tb = ScatterTable();
+    tb.t0 = t0;
+    tb.t1 = t1;
+}
+
+template <typename Tp>
+int talloc(mm_tomo* h, ScatterTable& tb, Tp** p, size_t count, const char* what) {
+    MM_TRY(alloc(h, p, count, what));
+    tb.bytes += count * sizeof(Tp);
+    return MM_OK;
+}
+
+constexpr int kBuildBytesPerTap = 26;  // keys (2 x 8), merge flags, positions, sort/scan temp
+
+// Builds the table of the angles [tb.t0, tb.t1): every tap of every sample
+// gets the key (pair << 33) | (tap offset in the block << 1) | half for its
+// destination cell; sorted, the taps of one cell pair come in sample order
+// and a left-cell tap followed by the same sample's right-cell tap merges
+// into one entry.
+int build_table(mm_tomo* h, ScatterTable& tb, cudaStream_t st) {
     const int n = h->n, T = h->ntheta, M = h->m, L = 2 * M + 1;
-    const long nent = (long)T * h->K * L * L;
+    const long per_angle = (long)h->K * L * L;
+    const long nent = (long)(tb.t1 - tb.t0) * per_angle, e0 = (long)tb.t0 * per_angle;
     const long npairs = 2L * n * (n / 2 + 1);
     MM_REQUIRE(nent < (1L << 32) && (long)T * h->K < (1L << 30), "adjoint table too large: %ld entries", nent);
     int pairbits = 1;
@@ -394,28 +445,32 @@ int build_csr(mm_tomo* h, cudaStream_t st) {
         for (void* b : bufs)
             if (b) cudaFree(b);
     };
-    auto fail_cuda = [&](cudaError_t e) {
+    auto fail = [&](int r) {
         cleanup();
-        mm::set_error("building the adjoint scatter table: %s", cudaGetErrorString(e));
-        return MM_ECUDA;
+        free_table(h, tb);
+        return r;
     };
-    if ((rc = dev_alloc((void**)&kin, nent * 8, "scatter keys")) != MM_OK) return cleanup(), rc;
-    if ((rc = dev_alloc((void**)&kout, nent * 8, "scatter keys (sorted)")) != MM_OK) return cleanup(), rc;
-    if ((rc = dev_alloc((void**)&head, nent * 4, "scatter merge flags")) != MM_OK) return cleanup(), rc;
-    if ((rc = dev_alloc((void**)&pos, nent * 4, "scatter entry positions")) != MM_OK) return cleanup(), rc;
+    auto fail_cuda = [&](cudaError_t e) {
+        mm::set_error("building the adjoint scatter table: %s", cudaGetErrorString(e));
+        return fail(MM_ECUDA);
+    };
+    if ((rc = dev_alloc((void**)&kin, nent * 8, "scatter keys")) != MM_OK) return fail(rc);
+    if ((rc = dev_alloc((void**)&kout, nent * 8, "scatter keys (sorted)")) != MM_OK) return fail(rc);
+    if ((rc = dev_alloc((void**)&head, nent * 4, "scatter merge flags")) != MM_OK) return fail(rc);
+    if ((rc = dev_alloc((void**)&pos, nent * 4, "scatter entry positions")) != MM_OK) return fail(rc);
     cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, kin, kout, (int64_t)nent, 0, 33 + pairbits, st);
     cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, head, pos, (int64_t)nent, st);
     tmp_bytes = std::max(tmp_bytes, scan_bytes);
-    if ((rc = dev_alloc(&tmp, tmp_bytes, "sort/scan temp")) != MM_OK) return cleanup(), rc;
+    if ((rc = dev_alloc(&tmp, tmp_bytes, "sort/scan temp")) != MM_OK) return fail(rc);
     const long gb = (nent + kThreads - 1) / kThreads;
     const float scale = (float)(1.0 / (4.0 * n * (double)n));
-#define MM_K(MM)                                                                     \
-    case MM:                                                                         \
-        k_pair_keys<MM><<<gb, kThreads, 0, st>>>(kin, h->d_cos, h->d_sin, n, T, nent); \
+#define MM_K(MM)                                                                         \
+    case MM:                                                                             \
+        k_pair_keys<MM><<<gb, kThreads, 0, st>>>(kin, h->d_cos, h->d_sin, n, T, nent, e0); \
         break;
     switch (M) {
         MM_K(2) MM_K(3) MM_K(4) MM_K(5) MM_K(6)
-        default: cleanup(); MM_REQUIRE(false, "unsupported m=%d", M);
+        default: mm::set_error("unsupported m=%d", M); return fail(MM_EINVAL);
     }
 #undef MM_K
     cudaError_t e = cudaGetLastError();
@@ -435,25 +490,28 @@ int build_csr(mm_tomo* h, cudaStream_t st) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail_cuda(e);
     const long nnz = (long)last_pos + last_head;
-    if ((rc = alloc(h, &h->csr_ptr, npairs + 1, "scatter pair pointers")) != MM_OK) return cleanup(), rc;
-    if ((rc = alloc(h, &h->csr_idx, nnz, "scatter sample index")) != MM_OK) return cleanup(), rc;
-    if ((rc = alloc(h, &h->csr_w, nnz, "scatter weights")) != MM_OK) return cleanup(), rc;
-    if ((rc = dev_alloc((void**)&pairs, nnz * 4, "scatter entry pairs")) != MM_OK) return cleanup(), rc;
-#define MM_P(MM)                                                                                               \
-    case MM:                                                                                                   \
-        k_pair_payload<MM><<<gb, kThreads, 0, st>>>(kout, head, pos, h->csr_idx, h->csr_w, pairs, h->d_cos,    \
-                                                    h->d_sin, n, T, nent, h->c0, h->c1, scale);                \
+    if ((rc = talloc(h, tb, &tb.ptr, npairs + 1, "scatter pair pointers")) != MM_OK) return fail(rc);
+    if ((rc = talloc(h, tb, &tb.idx, std::max(nnz, 1L), "scatter sample index")) != MM_OK) return fail(rc);
+    if ((rc = talloc(h, tb, &tb.w, std::max(nnz, 1L), "scatter weights")) != MM_OK) return fail(rc);
+    if ((rc = dev_alloc((void**)&pairs, std::max(nnz, 1L) * 4, "scatter entry pairs")) != MM_OK) return fail(rc);
+#define MM_P(MM)                                                                                                 \
+    case MM:                                                                                                     \
+        k_pair_payload<MM><<<gb, kThreads, 0, st>>>(kout, head, pos, tb.idx, tb.w, pairs, h->d_cos, h->d_sin, n, T, \
+                                                    nent, e0, h->c0, h->c1, scale);                              \
         break;
     switch (M) { MM_P(2) MM_P(3) MM_P(4) MM_P(5) MM_P(6) }
 #undef MM_P
-    k_pair_ptr<<<(nnz + 1 + kThreads - 1) / kThreads, kThreads, 0, st>>>(pairs, h->csr_ptr, nnz, npairs);
+    k_pair_ptr<<<(nnz + 1 + kThreads - 1) / kThreads, kThreads, 0, st>>>(pairs, tb.ptr, nnz, npairs);
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail_cuda(e);
     cleanup();
+    kin = kout = nullptr;
+    head = pos = pairs = nullptr;
+    tmp = nullptr;
     // long lists -> pieces of kChunk entries (fixed split: deterministic)
     std::vector<unsigned> hp(npairs + 1);
-    MM_CUDA(cudaMemcpy(hp.data(), h->csr_ptr, hp.size() * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    MM_CUDA(cudaMemcpy(hp.data(), tb.ptr, hp.size() * sizeof(unsigned), cudaMemcpyDeviceToHost));
     std::vector<uint2> tasks;
     std::vector<uint4> longp;
     for (long q = 0; q < npairs; ++q) {
@@ -464,17 +522,73 @@ int build_csr(mm_tomo* h, cudaStream_t st) {
         longp.push_back(make_uint4((unsigned)q, t0, (unsigned)tasks.size(), 0u));
     }
     if (!longp.empty()) {
-        MM_TRY(alloc(h, &h->chunk_task, tasks.size(), "scatter pieces"));
-        MM_TRY(alloc(h, &h->chunk_pair, longp.size(), "scatter long pairs"));
-        MM_TRY(alloc(h, &h->chunk_part, tasks.size() * 2 * (size_t)h->zs, "scatter partial sums"));
-        MM_CUDA(cudaMemcpy(h->chunk_task, tasks.data(), tasks.size() * sizeof(uint2), cudaMemcpyHostToDevice));
-        MM_CUDA(cudaMemcpy(h->chunk_pair, longp.data(), longp.size() * sizeof(uint4), cudaMemcpyHostToDevice));
+        if ((rc = talloc(h, tb, &tb.chunk_task, tasks.size(), "scatter pieces")) != MM_OK ||
+            (rc = talloc(h, tb, &tb.chunk_pair, longp.size(), "scatter long pairs")) != MM_OK ||
+            (rc = talloc(h, tb, &tb.chunk_part, tasks.size() * 2 * (size_t)h->zs, "scatter partial sums")) != MM_OK)
+            return fail(rc);
+        if (cudaMemcpy(tb.chunk_task, tasks.data(), tasks.size() * sizeof(uint2), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(tb.chunk_pair, longp.data(), longp.size() * sizeof(uint4), cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail_cuda(cudaGetLastError());
     }
-    h->nchunks = (long)tasks.size();
-    h->nlong = (long)longp.size();
-    h->nnz = nnz;
+    tb.nchunks = (long)tasks.size();
+    tb.nlong = (long)longp.size();
+    tb.nnz = nnz;
+    return MM_OK;
+}
+
+// Splits the angles into table blocks and decides whether the tables stay
+// resident: each block's build needs about kBuildBytesPerTap bytes per tap,
+// the blocks' tables together about 7 bytes per tap plus one pointer array
+// (4 bytes per cell pair) each.  The blocks are sized to a third of the free
+// device memory (and to opts.max_table_angles); when all their tables would
+// take more than half of it they are built at every RT call instead.
+int build_csr(mm_tomo* h, cudaStream_t st) {
+    if (h->csr_ready) return MM_OK;
+    const int T = h->ntheta, L = 2 * h->m + 1;
+    const long per_angle = (long)h->K * L * L;
+    const long npairs = 2L * h->n * (h->n / 2 + 1);
+    size_t freeb = 0, totalb = 0;
+    MM_CUDA(cudaMemGetInfo(&freeb, &totalb));
+    long tb = std::max(1L, std::min((long)T, ((1L << 32) - 1) / per_angle));
+    tb = std::max(1L, std::min(tb, (long)(freeb / 3 / kBuildBytesPerTap) / per_angle));
+    if (h->table_angles > 0) tb = std::min(tb, (long)h->table_angles);
+    const long nblocks = (T + tb - 1) / tb;
+    const double resident = 7.0 * per_angle * T + 4.0 * (npairs + 1) * nblocks;
+    h->tables_resident = resident <= 0.5 * (double)freeb;
+    h->tabs.assign(nblocks, ScatterTable());
+    for (long b = 0; b < nblocks; ++b) {
+        h->tabs[b].t0 = (int)(b * tb);
+        h->tabs[b].t1 = (int)std::min((long)T, (b + 1) * tb);
+    }
+    if (h->tables_resident) {
+        h->tm.begin(12, st);
+        for (auto& t : h->tabs) {
+            const int rc = build_table(h, t, st);
+            if (rc != MM_OK) {
+                for (auto& u : h->tabs) free_table(h, u);
+                h->tabs.clear();
+                return rc;
+            }
+        }
+        h->tm.end(st, 4 * (int)h->tabs.size());
+    }
     h->csr_ready = true;
-    h->tm.end(st, 4);
+    return MM_OK;
+}
+
+// The scatter of all angle blocks into A, in block order: the first block's
+// sums are stored, every later block's are added.
+int launch_scatter(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) {
+    for (size_t b = 0; b < h->tabs.size(); ++b) {
+        ScatterTable& t = h->tabs[b];
+        if (!h->tables_resident) MM_TRY(build_table(h, t, st));
+        const int rc = launch_table(h, t, Q, A, b > 0 ? 1 : 0, st);
+        if (!h->tables_resident) {
+            cudaStreamSynchronize(st);
+            free_table(h, t);
+        }
+        MM_TRY(rc);
+    }
     return MM_OK;
 }
 
@@ -482,5 +596,10 @@ int build_csr(mm_tomo* h, cudaStream_t st) {
 
 namespace mmtomo {
 int build_csr(mm_tomo* h, cudaStream_t st) { return ::build_csr(h, st); }
+void free_tables(mm_tomo* h) {
+    for (auto& t : h->tabs) ::free_table(h, t);
+    h->tabs.clear();
+    h->csr_ready = false;
+}
 int launch_scatter(mm_tomo* h, const float2* Q, float2* A, cudaStream_t st) { return ::launch_scatter(h, Q, A, st); }
 }  // namespace mmtomo

@@ -2,11 +2,14 @@
 
 The reference streams the padded (ntheta, 2nz, 2n) work buffer through pinned
 host memory in three separable passes (propagation_large.py:36-53).  On a
-B200 the propagator's separable two-pass kernels run device-resident, so this
-class keeps the host-array API -- numpy (or a banded pinned object with
+B200 the propagator's kernels run device-resident on chunks of frames, so
+this class keeps the host-array API -- numpy (or a banded pinned object with
 ``copy_to``) in, an internal pinned numpy buffer out, reused by the next call
 (propagation_large.py:226-236) -- and validates the chunk sizes with the same
-assertions (:216-223).
+assertions (:216-223).  Frames are streamed: the copy-in of chunk i+1, D of
+chunk i and the copy-out of chunk i-1 overlap on three streams
+(``staging.ChunkStream``); the chunk is sized from the free device memory
+(a 24576^2 frame, the reference scripts' ups = 8 size, is 4.8 GB).
 """
 from __future__ import annotations
 
@@ -15,6 +18,14 @@ import torch
 
 from model_mosaic_b200._interop import pinned_empty, require_cuda
 from model_mosaic_b200.processing.propagation import Propagation
+from model_mosaic_b200.staging import ChunkStream
+
+
+def chunk_frames(n, nz, ntheta, free_bytes):
+    """Frames per chunk: two device buffers per side plus the handle's two
+    work frames within about 40% of the free device memory."""
+    per = 8.0 * n * nz * 6
+    return max(1, min(ntheta, int(0.4 * free_bytes / per)))
 
 
 class PropagationLarge:
@@ -27,20 +38,30 @@ class PropagationLarge:
         self._prop_nt = 0
         self._out = None
         self._psi = None
+        self._stream = None
 
     def _engine(self, ntheta):
-        if self._prop is None or self._prop_nt < ntheta:
+        """A handle for chunks of frames (at most ntheta), sized by memory."""
+        free = torch.cuda.mem_get_info()[0] + (8 * self.n * self.nz * 2 * self._prop_nt if self._prop else 0)
+        want = chunk_frames(self.n, self.nz, ntheta, free)
+        if self._prop is None or self._prop_nt != want:
             if self._prop is not None:
                 self._prop.free()
-            self._prop_nt = ntheta
-            self._prop = Propagation(self.n, self.nz, ntheta, self.distance.size, self.wavelength,
+                self._prop = None
+            self._prop_nt = want
+            self._prop = Propagation(self.n, self.nz, want, self.distance.size, self.wavelength,
                                      self.voxelsize, self.distance)
+        if self._stream is None:
+            self._stream = ChunkStream()
         return self._prop
 
     def free(self):
         if self._prop is not None:
             self._prop.free()
         self._prop = None
+        if self._stream is not None:
+            self._stream.free()
+        self._stream = None
         self._out = self._psi = None
 
     def psi_buffer(self, ntheta):
@@ -68,10 +89,20 @@ class PropagationLarge:
         if self._out is None or self._out.shape != shape:
             self._out = pinned_empty(shape, np.complex64)
         prop = self._engine(ntheta)
-        x = torch.from_numpy(np.ascontiguousarray(psi, dtype=np.complex64)).cuda()
-        y = torch.empty_like(x)
-        (prop.DT_into if adjoint else prop.D_into)(x, y, j)
-        self._out[...] = y.cpu().numpy()
+        step = self._prop_nt
+        chunks_t = [(t0, min(ntheta, t0 + step)) for t0 in range(0, ntheta, step)]
+        out = self._out
+        run = prop.DT_into if adjoint else prop.D_into
+
+        def load(k, dst):
+            dst[...] = psi[k[0]:k[1]]
+
+        def store(k, src):
+            out[k[0]:k[1]] = src
+
+        fshape = lambda k: (k[1] - k[0], self.nz, self.n)  # noqa: E731
+        self._stream.run(chunks_t, fshape, np.complex64, fshape, np.complex64, load,
+                         lambda k, x, y: run(x, y, j), store)
         return self._out[0] if added else self._out
 
     def D(self, psi, j, chunks):

@@ -34,7 +34,7 @@ from model_mosaic_b200._interop import (require_cuda, to_device, from_device, st
 
 class _TomoOpts(C.Structure):
     _fields_ = [("eps", C.c_double), ("m", C.c_int), ("clamp_xy", C.c_int), ("compensated", C.c_int),
-                ("reserved", C.c_int * 4)]
+                ("max_table_angles", C.c_int), ("reserved", C.c_int * 3)]
 
 
 def _storage(dt: torch.dtype) -> int:
@@ -137,7 +137,9 @@ class TomoReal:
         return out
 
     def RT_into(self, y: torch.Tensor, out: torch.Tensor):
-        _ffi.check(_ffi.lib().mm_tomo_RT(self._handle(), C.c_void_p(y.data_ptr()), _ffi.MM_F32,
+        """float32 or complex64 sinogram y -> out of the same dtype."""
+        dt = _ffi.MM_C64 if y.is_complex() else _ffi.MM_F32
+        _ffi.check(_ffi.lib().mm_tomo_RT(self._handle(), C.c_void_p(y.data_ptr()), dt,
                                          C.c_void_p(out.data_ptr()), y.shape[1],
                                          C.c_void_p(stream_ptr(y.device))), "mm_tomo_RT")
         return out

@@ -2,10 +2,15 @@
 
 The reference stages its (nz, 2n, n+1) spectrum through pinned host memory
 because it did not fit on the GPUs it targeted (processing/tomo_large.py:1-19).
-A B200 holds every configuration of the forward model in HBM, so this class
+A B200 holds a slab of slices of the forward model in HBM, so this class
 keeps the reference's host-array API -- numpy in, numpy out, results in
 internal pinned buffers that the next call reuses (tomo_large.py:545-555,
-611) -- and runs the same device-resident USFFT as ``TomoReal`` in between.
+611) -- and runs the same device-resident USFFT as ``TomoReal`` on slabs of
+slices, streamed: the copy-in of slab i+1, the transform of slab i and the
+copy-out of slab i-1 overlap on three streams (``staging.ChunkStream``, as
+the reference's StreamPipe, processing/pipeline.py:255-359).  The slab is
+sized from the free device memory (a 24576^2 slice, the reference scripts'
+ups = 8 size, takes about 30 GB of workspace).
 
     tomo = TomoLargeReal(n, theta, chunk_xy)
     sino = tomo.R(obj_host, [chunk_n, chunk_theta, chunk_xy])
@@ -23,6 +28,20 @@ import torch
 
 from model_mosaic_b200._interop import pinned_empty, require_cuda
 from model_mosaic_b200.processing.tomo import TomoReal
+from model_mosaic_b200.staging import ChunkStream
+
+
+def slab_slices(n, ntheta, nz, max_nz, free_bytes):
+    """Slices per slab: a power of two (the handle pads slabs to one) whose
+    workspace -- the two (2n, n+1) spectra, the cuFFT x-side rows, the polar
+    lines, the scatter table share and the streamed buffers -- fits in
+    about half of the free device memory."""
+    per_slice = 8.0 * 2 * n * (n + 1) * 2 + 4.0 * n * 2 * n + 8.0 * n * (n + 1) + 12.0 * ntheta * n * 2 + 16.0 * n * n
+    fit = max(1, int(0.5 * free_bytes / per_slice))
+    z = 1
+    while z * 2 <= min(max_nz, nz, fit):
+        z *= 2
+    return z
 
 
 class TomoLargeReal:
@@ -39,13 +58,20 @@ class TomoLargeReal:
         self._sino = None
         self._obj = None
         self._obj_rt = None
+        self._stream = None
 
     def _engine(self, nz):
-        if self._tomo is None or self._tomo_nz < nz:
+        """A TomoReal handle for slabs of up to `nz` slices, sized by memory."""
+        want = slab_slices(self.n, self.ntheta, nz, self._max_nz, torch.cuda.mem_get_info()[0]
+                           + (self._tomo.workspace_bytes() if self._tomo is not None else 0))
+        if self._tomo is None or self._tomo_nz != want:
             if self._tomo is not None:
                 self._tomo.free()
-            self._tomo_nz = max(nz, 1)
-            self._tomo = TomoReal(self.n, self._tomo_nz, self.theta, eps=self._eps, m=self._m, clamp_xy=True)
+                self._tomo = None
+            self._tomo_nz = want
+            self._tomo = TomoReal(self.n, want, self.theta, eps=self._eps, m=self._m, clamp_xy=True)
+        if self._stream is None:
+            self._stream = ChunkStream()
         return self._tomo
 
     def _check_chunks(self, chunks):
@@ -58,6 +84,9 @@ class TomoLargeReal:
         if self._tomo is not None:
             self._tomo.free()
         self._tomo = None
+        if self._stream is not None:
+            self._stream.free()
+        self._stream = None
         self._sino = self._obj = self._obj_rt = None
 
     def obj_buffer(self, nz):
@@ -73,18 +102,23 @@ class TomoLargeReal:
         returned in an internal buffer valid until the next R()."""
         self._check_chunks(chunks)
         obj = np.asarray(obj)
-        nz = obj.shape[0]
-        shape = (self.ntheta, nz, self.n)
+        nz, n, T = obj.shape[0], self.n, self.ntheta
+        shape = (T, nz, n)
         if self._sino is None or self._sino.shape != shape:
             self._sino = pinned_empty(shape, np.float32)
-        tomo = self._engine(min(nz, self._max_nz) if nz > self._max_nz else nz)
+        tomo = self._engine(nz)
         step = tomo._nz
-        for z0 in range(0, nz, step):
-            z1 = min(nz, z0 + step)
-            x = torch.from_numpy(np.ascontiguousarray(obj[z0:z1], dtype=np.float32)).cuda()
-            out = torch.empty((self.ntheta, z1 - z0, self.n), dtype=torch.float32, device="cuda")
-            tomo.R_into(x, out)
-            self._sino[:, z0:z1, :] = out.cpu().numpy()
+        slabs = [(z0, min(nz, z0 + step)) for z0 in range(0, nz, step)]
+        sino = self._sino
+
+        def load(k, dst):
+            dst[...] = obj[k[0]:k[1]]
+
+        def store(k, src):
+            sino[:, k[0]:k[1], :] = src
+
+        self._stream.run(slabs, lambda k: (k[1] - k[0], n, n), np.float32, lambda k: (T, k[1] - k[0], n),
+                         np.float32, load, lambda k, x, y: tomo.R_into(x, y), store)
         return self._sino
 
     def RT(self, sino, chunks):
@@ -92,15 +126,22 @@ class TomoLargeReal:
         obj of the matching dtype, in an internal buffer (tomo_large.py:582-630)."""
         self._check_chunks(chunks)
         sino = np.asarray(sino)
-        nz = sino.shape[1]
+        T, nz, n = sino.shape[0], sino.shape[1], self.n
         dt = np.complex64 if np.iscomplexobj(sino) else np.float32
-        shape = (nz, self.n, self.n)
+        shape = (nz, n, n)
         if self._obj_rt is None or self._obj_rt.shape != shape or self._obj_rt.dtype != dt:
             self._obj_rt = pinned_empty(shape, dt)
-        tomo = self._engine(min(nz, self._max_nz) if nz > self._max_nz else nz)
+        tomo = self._engine(nz)
         step = tomo._nz
-        for z0 in range(0, nz, step):
-            z1 = min(nz, z0 + step)
-            part = np.ascontiguousarray(sino[:, z0:z1, :], dtype=dt)
-            self._obj_rt[z0:z1] = tomo.RT(part)
+        slabs = [(z0, min(nz, z0 + step)) for z0 in range(0, nz, step)]
+        out = self._obj_rt
+
+        def load(k, dst):
+            dst[...] = sino[:, k[0]:k[1], :]
+
+        def store(k, src):
+            out[k[0]:k[1]] = src
+
+        self._stream.run(slabs, lambda k: (T, k[1] - k[0], n), dt, lambda k: (k[1] - k[0], n, n), dt, load,
+                         lambda k, x, y: tomo.RT_into(x, y), store)
         return self._obj_rt
