@@ -16,7 +16,8 @@ Keyword-only extras (not in the reference): ``eps`` and ``m`` override the
 Gaussian accuracy / half-width (defaults 1e-3 and 4, processing/tomo.py:39-42);
 ``clamp_xy`` selects TomoLargeReal's clamped sample coordinates
 (processing/kernels.py:478-481); ``compensated`` makes the adjoint's sums
-Kahan-compensated.  bfloat16 torch tensors are accepted as storage (the
+Kahan-compensated; ``max_table_angles`` caps the angles per block of the
+adjoint's scatter table (0: sized by free device memory).  bfloat16 torch tensors are accepted as storage (the
 arithmetic stays float32): ``R`` of a bfloat16 volume returns a bfloat16
 sinogram unless ``out_dtype`` says otherwise, ``RT`` of a bfloat16 sinogram
 returns a bfloat16 volume.
@@ -45,7 +46,7 @@ class TomoReal:
     """Radon transform via USFFT for REAL float32 objects (processing/tomo.py:17)."""
 
     def __init__(self, n, nz, theta, *, eps: float = 1e-3, m: int | None = None, clamp_xy: bool = False,
-                 compensated: bool = False):
+                 compensated: bool = False, max_table_angles: int = 0):
         require_cuda()
         L = _ffi.lib()
         self.n = int(n)
@@ -54,7 +55,7 @@ class TomoReal:
         self.ntheta = len(th)
         self.theta = th
         opts = _TomoOpts(eps=float(eps), m=int(m or 0), clamp_xy=int(bool(clamp_xy)),
-                         compensated=int(bool(compensated)))
+                         compensated=int(bool(compensated)), max_table_angles=int(max_table_angles))
         h = C.c_void_p()
         _ffi.check(L.mm_tomo_create(self.n, self._nz, self.ntheta, th.ctypes.data_as(C.c_void_p),
                                     C.byref(opts), C.byref(h)), "mm_tomo_create")

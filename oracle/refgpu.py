@@ -12,7 +12,8 @@ method follows the reference line by line:
 
 * RefGpuTomoReal.R ........ processing/tomo.py:121-151
 * RefGpuTomoReal.RT ....... processing/tomo.py:153-188 (atomic scatter)
-* RefGpuPropagation.D ..... processing/propagation.py:36-64
+* RefGpuPropagation.D ..... processing/propagation.py:36-64 (beyond the pad
+  kernel's 32-bit index range, the same mirror padding with torch gathers)
 * psi / |.|^2 ............. step3_propagation.py:94-110 (element-wise)
 
 It serves three purposes: GPU parity of the product against the reference's
@@ -36,6 +37,16 @@ from .fresnel import fresnel_kernel, mirror_index
 
 _PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "libref_gpu.so")
 _LIB = None
+_INT_MAX = 2 ** 31 - 1
+
+
+def _need_int32(what: str, count: int):
+    """The reference's kernels compute element offsets in 32-bit int: past
+    2^31 - 1 they address memory outside their buffers (at n = 24576 its
+    scatter wrote out of bounds and its pad kernel made an illegal access).
+    Such sizes are refused instead of run."""
+    if count > _INT_MAX:
+        raise ValueError(f"{what}: {count} elements exceed the reference kernel's 32-bit indexing")
 
 
 def available() -> bool:
@@ -86,6 +97,8 @@ class RefGpuTomoReal:
         c2 = (1 - 2 * (np.arange(1, 2 * self.n + 1) % 2)).astype(np.float32)
         self.c2d = torch.from_numpy(np.outer(c2, c2)).to(dev)
         n = self.n
+        _need_int32("gather_rfft_full spectrum", self._nz * 2 * n * (n + 1))
+        _need_int32("gather_rfft_full sinogram", self.ntheta * self._nz * n)
         self._buf_padded = torch.zeros((self._nz, 2 * n, 2 * n), dtype=torch.float32, device=dev)
         self._buf_sino = torch.zeros((self.ntheta, self._nz, n), dtype=torch.complex64, device=dev)
         self._buf_fde_full = None
@@ -108,6 +121,7 @@ class RefGpuTomoReal:
     def RT(self, data: torch.Tensor) -> torch.Tensor:
         """tomo.py:153-188: full complex path with the atomic scatter."""
         n, nz = self.n, data.shape[1]
+        _need_int32("gather (dir=1) full spectrum", self._nz * 2 * n * 2 * n)
         if self._buf_fde_full is None:                                        # _lazy_init_rt, :90-107
             self._buf_fde_full = torch.zeros((self._nz, 2 * n, 2 * n), dtype=torch.complex64,
                                              device=self.theta.device)
@@ -148,8 +162,13 @@ class RefGpuPropagation:
         nt, n, nz = psi.shape[0], self.n, self.nz
         psi = psi.contiguous()
         self._buf_big.zero_()
-        _launch(lib().refgpu_pad_fwd, (math.ceil(2 * n / 32), math.ceil(2 * nz / 32), nt), (32, 32, 1),
-                _p(self._buf_big), _p(psi), n, nz, nt)
+        if nt * 2 * nz * 2 * n <= _INT_MAX:
+            _launch(lib().refgpu_pad_fwd, (math.ceil(2 * n / 32), math.ceil(2 * nz / 32), nt), (32, 32, 1),
+                    _p(self._buf_big), _p(psi), n, nz, nt)
+        else:
+            # beyond the pad kernel's 32-bit indexing: the same mirror padding
+            # (kernels.py:541-544) with torch's 64-bit gathers
+            self._buf_big[:nt] = psi.index_select(1, self.iy).index_select(2, self.ix)
         f = torch.fft.fft2(self._buf_big, dim=(-2, -1))
         f *= self.fker[j]
         f = torch.fft.ifft2(f, dim=(-2, -1), norm="forward")

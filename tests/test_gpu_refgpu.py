@@ -66,6 +66,18 @@ def test_D_vs_reference_gpu_kernels():
     assert err < RTOL
 
 
+def test_reference_pad_by_gathers_matches_its_kernel():
+    # beyond the pad kernel's 32-bit indexing RefGpuPropagation pads with torch
+    # gathers; where the kernel is in range the two must agree bit for bit
+    n, nz, T = 96, 40, 3
+    p = refgpu.RefGpuPropagation(n, nz, T, 1, 4.133e-11, 0.69e-6, [0.12])
+    gen = torch.Generator(device="cuda").manual_seed(14)
+    psi = torch.complex(torch.randn((T, nz, n), generator=gen, device="cuda"),
+                        torch.randn((T, nz, n), generator=gen, device="cuda"))
+    p.D(psi, 0)
+    assert torch.equal(p._buf_big[:T], psi.index_select(1, p.iy).index_select(2, p.ix))
+
+
 def test_reference_DT_is_adjoint():
     n, nz, T = 256, 32, 4
     p = refgpu.RefGpuPropagation(n, nz, T, 1, 4.133e-11, 0.69e-6, [0.12])
