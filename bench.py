@@ -48,6 +48,11 @@ WORKLOADS = {
     # the production slice size (4096-point columns, 2048-point rows) on ~4.5 GB
     "profile2048": dict(n=2048, nz=32, ntheta=128, theta_max=2 * np.pi, energy_kev=30.0,
                         distance=0.12, voxelsize=0.69e-6),
+    # the production layout (64 slices of 2048^2: the same column, gather and
+    # D kernels, per-launch column traffic independent of the angle count) on
+    # ~9.5 GB, few angles
+    "profile64": dict(n=2048, nz=64, ntheta=64, theta_max=2 * np.pi, energy_kev=30.0,
+                      distance=0.12, voxelsize=0.69e-6),
 }
 BETA_RATIO = 100.0
 L2_BYTES = 126 * 2 ** 20
