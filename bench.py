@@ -291,10 +291,14 @@ def run_ours(args, w, rank, world, local_rank):
     t_launch = own[top][0] / max(1, own[top][1])
     peak, peak_kind = peaks()
     achieved = alg[top] / (t_launch * 1e-3) / 1e9
-    kname = {"gather": "k_gather", "pad_phi": "k_xfwd", "y_fft": "k_col_fft", "r_c2r": "k_rc2r",
+    col_kernel = "k_col_l2" if (n == 2048 and nz % 8 == 0) else "k_col_fft"   # tomo_col.cu covers 2n = 4096
+    kname = {"gather": "k_gather", "pad_phi": "k_xfwd", "y_fft": col_kernel, "r_c2r": "k_rc2r",
              "y_pass": "k_ypass", "x_pass": "k_xpass"}[top]
     traffic = profile_traffic(args.workload, kname)
-    step_bytes = sum(alg.values())
+    # the step's algorithmic bytes as the hot-path scope defines them: R's
+    # B_R = 4V + 16Hc + 16H + 4S and D's B_D = 24P (Hc = nz n (n+1))
+    Hc = nz * n * (n + 1)
+    step_bytes = (4 * V + 16 * Hc + 16 * H + 4 * T * nz * n) + 24 * P
     roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak,
             "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "traffic": traffic, "alg_bytes_per_launch": alg[top], "ms_per_launch": round(t_launch, 4)}
