@@ -53,6 +53,10 @@ WORKLOADS = {
     # ~9.5 GB, few angles
     "profile64": dict(n=2048, nz=64, ntheta=64, theta_max=2 * np.pi, energy_kev=30.0,
                       distance=0.12, voxelsize=0.69e-6),
+    # step8_fbp.py's default size (n = 3072, 3n/4 = 2304 angles on [0, pi)):
+    # 6144-point columns and rows, 1536-point r-side lines (radix-3 passes)
+    "n3072": dict(n=3072, nz=32, ntheta=2304, theta_max=np.pi, energy_kev=30.0,
+                  distance=0.12, voxelsize=0.69e-6),
 }
 BETA_RATIO = 100.0
 L2_BYTES = 126 * 2 ** 20

@@ -34,12 +34,15 @@ struct mm_fbp {
 namespace {
 
 // Two rows per block: r0 = 2*blockIdx.x in the real part, r0 + 1 in the
-// imaginary part (zero when absent).  Bounded to 64 registers so that 1024
-// threads share an SM (two 8192-point lines): faster than one block at 128
-// registers despite a few spills.
+// imaginary part (zero when absent).  Powers of two: bounded to 64 registers
+// so that 1024 threads share an SM (two 8192-point lines), faster than one
+// block at 128 registers despite a few spills; 3 * 2^k lengths (24 values
+// per thread) at 128 registers.
 template <int L>
 __global__ void __launch_bounds__(stockham::Sched<L>::G,
-                                  stockham::Sched<L>::G >= 32 ? 1024 / stockham::Sched<L>::G : 32)
+                                  stockham::Sched<L>::P2
+                                      ? (stockham::Sched<L>::G >= 32 ? 1024 / stockham::Sched<L>::G : 32)
+                                      : 512 / (stockham::Sched<L>::G >= 32 ? stockham::Sched<L>::G : 32))
     k_fbp_filter(float* __restrict__ rows, long nrows,
                                                                       const float* __restrict__ w,
                                                                       const float2* __restrict__ tw, int n,
@@ -94,6 +97,14 @@ int dispatch_native(mm_fbp* h, float* rows, long nrows, const float* w, cudaStre
         case 2048: return launch_native<2048>(h, rows, nrows, w, st);
         case 4096: return launch_native<4096>(h, rows, nrows, w, st);
         case 8192: return launch_native<8192>(h, rows, nrows, w, st);
+        case 96: return launch_native<96>(h, rows, nrows, w, st);
+        case 192: return launch_native<192>(h, rows, nrows, w, st);
+        case 384: return launch_native<384>(h, rows, nrows, w, st);
+        case 768: return launch_native<768>(h, rows, nrows, w, st);
+        case 1536: return launch_native<1536>(h, rows, nrows, w, st);
+        case 3072: return launch_native<3072>(h, rows, nrows, w, st);
+        case 6144: return launch_native<6144>(h, rows, nrows, w, st);
+        case 12288: return launch_native<12288>(h, rows, nrows, w, st);
     }
     MM_REQUIRE(false, "FBP filter: no native kernel for ne=%d", h->ne);
 }
@@ -181,7 +192,9 @@ extern "C" int mm_fbp_create(int n, int batch_chunk, mm_fbp** out) {
     h->n = n;
     h->ne = 4 * n;
     h->chunk = batch_chunk;
-    h->native = mm_is_pow2(h->ne) && h->ne >= 16 && h->ne <= 8192;
+    // native padded lengths: powers of two in [16, 8192], 3 * 2^k in [96, 12288]
+    h->native = mm_is_pow2(h->ne) ? (h->ne >= 16 && h->ne <= 8192)
+                                  : (stockham::length_ok(h->ne) && h->ne >= 96 && h->ne <= 12288);
     int rc = MM_OK;
     if (h->native) {
         std::vector<float2> tw(4 * (size_t)h->ne, make_float2(0.f, 0.f));

@@ -1,4 +1,4 @@
-// Power-of-two FFTs held in registers, exchanged once through shared memory.
+// FFTs held in registers, exchanged through shared memory.
 //
 // A length L = R1*R2 transform is done in two register steps:
 //   x[R2*n1 + n2]  --R1-point FFT over n1, twiddle W_L^(n2*k1)-->  Y[k1][n2]
@@ -81,11 +81,71 @@ __device__ __forceinline__ void dit_layers(float2 (&v)[R]) {
     }
 }
 
-// In-register radix-2 FFT of size R <= 64, natural order in and out.
-// INV = false: exp(-2 pi i ...); INV = true: exp(+2 pi i ...), unnormalised.
+// W_12^j = exp(-2*pi*i*j/12) as compile-time constants (j folds to a
+// constant in unrolled code): the twiddles of the 3 * 2^a register FFTs.
+__host__ __device__ constexpr float2 w12(int j) {
+    constexpr float h = 0.86602540378443864676f;  // sqrt(3) / 2
+    switch (j % 12) {
+        case 0: return float2{1.f, 0.f};
+        case 1: return float2{h, -0.5f};
+        case 2: return float2{0.5f, -h};
+        case 3: return float2{0.f, -1.f};
+        case 4: return float2{-0.5f, -h};
+        case 5: return float2{-h, -0.5f};
+        case 6: return float2{-1.f, 0.f};
+        case 7: return float2{-h, 0.5f};
+        case 8: return float2{-0.5f, h};
+        case 9: return float2{0.f, 1.f};
+        case 10: return float2{0.5f, h};
+        default: return float2{h, 0.5f};
+    }
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void reg_fft(float2 (&v)[R]);
+
+// In-register FFT of size R = 3M (M = 1, 2, 4): with n = M n1 + n2 and
+// k = k1 + 3 k2, a 3-point DFT over n1 for each n2, the twiddle
+// W_R^(n2 k1), then an M-point FFT over n2 for each k1.
+template <int R, bool INV>
+__device__ __forceinline__ void reg_fft3(float2 (&v)[R]) {
+    constexpr int M = R / 3;
+    constexpr float h = 0.86602540378443864676f;
+    constexpr float sh = INV ? -h : h;
+    float2 y[3][M];
+#pragma unroll
+    for (int n2 = 0; n2 < M; ++n2) {
+        const float2 a = v[n2], b = v[M + n2], c = v[2 * M + n2];
+        const float2 t = make_float2(b.x + c.x, b.y + c.y), d = make_float2(b.x - c.x, b.y - c.y);
+        const float2 m = make_float2(a.x - 0.5f * t.x, a.y - 0.5f * t.y);
+        y[0][n2] = make_float2(a.x + t.x, a.y + t.y);
+        // forward: X1 = m - i h d, X2 = m + i h d (inverse: h -> -h)
+        float2 y1 = make_float2(m.x + sh * d.y, m.y - sh * d.x);
+        float2 y2 = make_float2(m.x - sh * d.y, m.y + sh * d.x);
+        if (n2 > 0) {
+            const float2 w1 = w12(n2 * (12 / R)), w2 = w12(2 * n2 * (12 / R));
+            y1 = INV ? cmulc(y1, w1) : cmul(y1, w1);
+            y2 = INV ? cmulc(y2, w2) : cmul(y2, w2);
+        }
+        y[1][n2] = y1;
+        y[2][n2] = y2;
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 3; ++k1) {
+        reg_fft<M, INV>(y[k1]);
+#pragma unroll
+        for (int k2 = 0; k2 < M; ++k2) v[k1 + 3 * k2] = y[k1][k2];
+    }
+}
+
+// In-register FFT of size R (a power of two <= 64, or 3, 6, 12), natural
+// order in and out.  INV = false: exp(-2 pi i ...); INV = true:
+// exp(+2 pi i ...), unnormalised.
 template <int R, bool INV>
 __device__ __forceinline__ void reg_fft(float2 (&v)[R]) {
-    if constexpr (R > 1) {
+    if constexpr (R % 3 == 0) {
+        reg_fft3<R, INV>(v);
+    } else if constexpr (R > 1) {
         float2 t[R];
 #pragma unroll
         for (int i = 0; i < R; ++i) t[i] = v[brev<R>(i)];
@@ -113,19 +173,22 @@ template <> struct Split<4096> { static constexpr int R1 = 64, R2 = 64; };
 }  // namespace mmfft
 
 // ---------------------------------------------------------------------------
-// Stockham radix-16 FFT of one line of length L held in shared memory.
+// Stockham FFT of one line of length L held in shared memory, L a power of
+// two or three times one.
 //
-// G = L/16 threads cooperate on a line (t in [0, G)); each holds 16 complex
-// values per pass.  Pass p has span NS = 16^p and radix RP = 16 except the
-// last, RP = L / 16^(P-1).  In a pass every group j = t + G*q reads
-// x[j + i*L/RP] (i < RP), multiplies by W_{NS*RP}^(i*(j mod NS)), does an
-// RP-point register FFT and writes y[(j/NS)*NS*RP + (j mod NS) + i*NS]:
-// natural order in, natural order out, no bit reversal.  The first pass reads
-// through `ld(pos)` and the last writes through `st(pos, value)`, so a
-// transform can start from global memory and end in global memory; the
-// passes in between use `buf` through the addressing functor `ad(pos)`.
-// Twiddles: per pass p >= 1 a table tw + off_p with W_{NS*RP}^(i*k) at
-// [i*NS + k]; lanes with consecutive j read consecutive entries.
+// Powers of two: G = L/16 threads cooperate on a line (t in [0, G)), each
+// holding V = 16 complex values per pass; pass p has span NS = 16^p and radix
+// RP = 16 except the last, RP = L / 16^(P-1).  L = 3 * 2^k: base radix 8 and
+// V = 24 values per thread (G = L/24), the last pass of radix 3, 6 or 12
+// (L / 8^(P-1)).  In a pass every group j = t + G*q reads x[j + i*L/RP]
+// (i < RP), multiplies by W_{NS*RP}^(i*(j mod NS)), does an RP-point
+// register FFT and writes y[(j/NS)*NS*RP + (j mod NS) + i*NS]: natural order
+// in, natural order out, no bit reversal.  The first pass reads through
+// `ld(pos)` and the last writes through `st(pos, value)`, so a transform can
+// start from global memory and end in global memory; the passes in between
+// use `buf` through the addressing functor `ad(pos)`.  Twiddles: per pass
+// p >= 1 a table tw + off_p with W_{NS*RP}^(i*k) at [i*NS + k]; lanes with
+// consecutive j read consecutive entries.
 namespace stockham {
 
 using mmfft::cmul;
@@ -133,18 +196,28 @@ using mmfft::cmulc;
 using mmfft::ilog2;
 using mmfft::reg_fft;
 
-// Schedule of a length-L line: passes of radix 16 and one smaller radix
-// (L not a power of 16), the small one last (REV = false) or first (REV =
-// true).  The inverse half of a convolution uses the reversed schedule so
-// that its first pass owns exactly the elements the forward's last pass
-// produced (see conv()).
+// Line lengths the engine covers: 2^k and 3 * 2^k.
+__host__ __device__ constexpr bool length_ok(long L) {
+    return L >= 2 && ((L & (L - 1)) == 0 || (L % 3 == 0 && ((L / 3) & (L / 3 - 1)) == 0));
+}
+
+// Schedule of a length-L line: passes of the base radix and one smaller
+// radix, the small one last (REV = false) or first (REV = true).  The
+// inverse half of a convolution uses the reversed schedule so that its first
+// pass owns exactly the elements the forward's last pass produced (see
+// conv()).
 template <int L, bool REV = false>
 struct Sched {
-    static constexpr int P = L <= 16 ? 1 : (ilog2<L>() + 3) / 4;   // passes
-    static constexpr int G = L >= 16 ? L / 16 : 1;                  // threads per line
-    static constexpr int V = L >= 16 ? 16 : L;                      // values per thread
-    static constexpr int small = L >> (4 * (P - 1));
-    static constexpr int radix(int p) { return REV ? (p == 0 ? small : 16) : (p < P - 1 ? 16 : small); }
+    static_assert(length_ok(L), "line length must be 2^k or 3 * 2^k");
+    static constexpr bool P2 = (L & (L - 1)) == 0;
+    static constexpr int B = P2 ? 16 : 8;                         // base radix
+    static constexpr int VB = P2 ? 16 : 24;                       // values per thread
+    static constexpr int K2 = ilog2<P2 ? L : L / 3>();            // exponent of the power-of-two factor
+    static constexpr int P = P2 ? (L <= 16 ? 1 : (K2 + 3) / 4) : 1 + K2 / 3;   // passes
+    static constexpr int G = L >= VB ? L / VB : 1;                // threads per line
+    static constexpr int V = L >= VB ? VB : L;                    // values per thread
+    static constexpr int small = P2 ? (L >> (4 * (P - 1))) : (L >> (3 * (P - 1)));
+    static constexpr int radix(int p) { return REV ? (p == 0 ? small : B) : (p < P - 1 ? B : small); }
     static constexpr int span(int p) {
         int s = 1;
         for (int q = 0; q < p; ++q) s *= radix(q);
@@ -159,16 +232,17 @@ struct Sched {
 };
 
 // Host-side table for Sched<L, rev> (FP64 angles), Sched<L, rev>::tw_size()
-// entries: pass p >= 1, W_{NS*RP}^(i*k) at [off_p + i*NS + k].
+// entries: pass p >= 1, W_{NS*RP}^(i*k) at [off_p + i*NS + k].  Returns the
+// entry count (at most 1.5 L), or -1 for a length the engine does not cover.
 inline int host_twiddles(int L, bool rev, float2* out) {
-    int P = 1;
-    if (L > 16) {
-        int lg = 0;
-        while ((1 << lg) < L) ++lg;
-        P = (lg + 3) / 4;
-    }
-    const int small = L >> (4 * (P - 1));
-    auto radix = [&](int p) { return rev ? (p == 0 ? small : 16) : (p < P - 1 ? 16 : small); };
+    if (!length_ok(L)) return -1;
+    const bool p2 = (L & (L - 1)) == 0;
+    int k2 = 0;
+    while ((1L << (k2 + 1)) <= (p2 ? L : L / 3)) ++k2;
+    const int P = p2 ? (L <= 16 ? 1 : (k2 + 3) / 4) : 1 + k2 / 3;
+    const int base = p2 ? 16 : 8;
+    const int small = p2 ? (L >> (4 * (P - 1))) : (L >> (3 * (P - 1)));
+    auto radix = [&](int p) { return rev ? (p == 0 ? small : base) : (p < P - 1 ? base : small); };
     int o = 0, ns = radix(0);
     for (int p = 1; p < P; ++p) {
         const int rp = radix(p);
@@ -192,7 +266,7 @@ struct PassShape {
     static constexpr int NS = S::span(PASS);
     static constexpr int NG = L / RP;
     static constexpr int Q = NG / S::G;
-    static_assert(Q * RP == S::V, "16 values per thread");
+    static_assert(Q * RP == S::V, "V values per thread in every pass");
 };
 
 template <int L, bool REV, int PASS, bool INV, class Src>
@@ -206,7 +280,7 @@ __device__ __forceinline__ void pass_load(float2 (&x)[PassShape<L, REV, PASS>::Q
 #pragma unroll
         for (int i = 0; i < Sh::RP; ++i) x[q][i] = src(j + i * Sh::NG);
         if (Sh::NS > 1) {
-            const int k = j & (Sh::NS - 1);
+            const int k = j % Sh::NS;
             const float2* tp = tw + S::tw_off(PASS);
 #pragma unroll
             for (int i = 1; i < Sh::RP; ++i) {
@@ -226,7 +300,7 @@ __device__ __forceinline__ void pass_store(float2 (&x)[PassShape<L, REV, PASS>::
 #pragma unroll
     for (int q = 0; q < Sh::Q; ++q) {
         const int j = t + S::G * q;
-        const int k = j & (Sh::NS - 1);
+        const int k = j % Sh::NS;
         const int base = (j / Sh::NS) * Sh::NS * Sh::RP + k;
 #pragma unroll
         for (int i = 0; i < Sh::RP; ++i) dst(base + i * Sh::NS, x[q][i]);
@@ -346,7 +420,7 @@ __device__ __forceinline__ void pairconv(float2* __restrict__ buf, const Ad& ad,
 #pragma unroll
         for (int i = 0; i < Sf::RP; ++i) {
             const int k = j + i * Sf::NG;
-            x[q][i] = pair(k, x[q][i], buf[ad((N - k) & (N - 1))]);
+            x[q][i] = pair(k, x[q][i], buf[ad(k == 0 ? 0 : N - k)]);
         }
         reg_fft<Sf::RP, true>(x[q]);
     }

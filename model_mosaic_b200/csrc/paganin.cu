@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(RPB * stockham::Sched<N>::G) k_pg_xfwd(const f
     __syncthreads();
     if (!live) return;
     for (int k = g; k < NH; k += G) {
-        const float2 z1 = sm[ad(k)], z2 = sm[ad((N - k) & (N - 1))];
+        const float2 z1 = sm[ad(k)], z2 = sm[ad(k == 0 ? 0 : N - k)];
         // Za = (Z[k] + conj Z[N-k]) / 2, Zb = (Z[k] - conj Z[N-k]) / (2i)
         spec[ra * NH + k] = make_float2(0.5f * (z1.x + z2.x), 0.5f * (z1.y - z2.y));
         if (hasb) spec[rb * NH + k] = make_float2(0.5f * (z1.y + z2.y), -0.5f * (z1.x - z2.x));
@@ -155,7 +155,7 @@ int launch_cols(const mm_pgn* h, int frames, cudaStream_t st) {
     return MM_OK;
 }
 
-#define MM_POW2_SWITCH(x, F, ...)                                              \
+#define MM_LINE_SWITCH(x, F, ...)                                              \
     switch (x) {                                                               \
         case 2: return F<2>(__VA_ARGS__);                                      \
         case 4: return F<4>(__VA_ARGS__);                                      \
@@ -169,18 +169,24 @@ int launch_cols(const mm_pgn* h, int frames, cudaStream_t st) {
         case 1024: return F<1024>(__VA_ARGS__);                                \
         case 2048: return F<2048>(__VA_ARGS__);                                \
         case 4096: return F<4096>(__VA_ARGS__);                                \
+        case 96: return F<96>(__VA_ARGS__);                                    \
+        case 192: return F<192>(__VA_ARGS__);                                  \
+        case 384: return F<384>(__VA_ARGS__);                                  \
+        case 768: return F<768>(__VA_ARGS__);                                  \
+        case 1536: return F<1536>(__VA_ARGS__);                                \
+        case 3072: return F<3072>(__VA_ARGS__);                                \
     }
 
 int rows_pass(const mm_pgn* h, bool inverse, const float* I, float* out, long rows, cudaStream_t st) {
-    MM_POW2_SWITCH(h->n, launch_rows, h, inverse, I, out, rows, st)
+    MM_LINE_SWITCH(h->n, launch_rows, h, inverse, I, out, rows, st)
     MM_REQUIRE(false, "Paganin: no native row kernel for n=%d", h->n);
 }
 
 int cols_pass(const mm_pgn* h, int frames, cudaStream_t st) {
-    MM_POW2_SWITCH(h->nz, launch_cols, h, frames, st)
+    MM_LINE_SWITCH(h->nz, launch_cols, h, frames, st)
     MM_REQUIRE(false, "Paganin: no native column kernel for nz=%d", h->nz);
 }
-#undef MM_POW2_SWITCH
+#undef MM_LINE_SWITCH
 
 // General sizes: the reference's rfft2 * H -> irfft2 over all ntheta frames
 // (tail frames zeroed), then -log(clip).
@@ -248,7 +254,9 @@ extern "C" int mm_pgn_create(int n, int nz, int ntheta, const float* filt_host, 
     h->nz = nz;
     h->ntheta = ntheta;
     h->nh = n / 2 + 1;
-    h->native = mm_is_pow2(n) && n <= 4096 && mm_is_pow2(nz) && nz <= 4096;
+    // native line lengths: powers of two up to 4096, 3 * 2^k in [96, 3072]
+    auto line_ok = [](int L) { return mm_is_pow2(L) ? L <= 4096 : (stockham::length_ok(L) && L >= 96 && L <= 3072); };
+    h->native = line_ok(n) && line_ok(nz);
     auto fail = [&](int rc) {
         destroy(h);
         return rc;

@@ -84,7 +84,8 @@ __device__ __forceinline__ float2 pair_mix(const float4* __restrict__ S, int k, 
 // G = nz/16 threads of each column's Stockham transform (fft_smem.cuh).
 // NXC: the row length n fixed at compile time (row offsets become immediates), 0 for runtime.
 template <int N, int CW, int IN, int NXC>
-__global__ void __launch_bounds__(CW * stockham::Sched<N>::G, 1024 / (CW * stockham::Sched<N>::G))
+__global__ void __launch_bounds__(CW * stockham::Sched<N>::G,
+                                  (stockham::Sched<N>::P2 ? 1024 : 512) / (CW * stockham::Sched<N>::G))
     k_ypass(const void* __restrict__ src, float2* __restrict__ dst, const float4* __restrict__ Sy,
             const float2* __restrict__ tw, int n_rt, float s, float ib) {
     const int n = NXC > 0 ? NXC : n_rt;
@@ -311,6 +312,12 @@ int launch_x(mm_prop* h, void* dst, int ntheta, const float4* S, cudaStream_t st
 }
 
 // Column pass of distance j; adj selects the conj(K) tables.
+// Line lengths with native kernels: powers of two in [2, 2048] and
+// 3 * 2^k in [96, 3072]; other sizes take the cuFFT path.
+bool native_len(int L) {
+    return mm_is_pow2(L) ? (L >= 2 && L <= 2048) : (stockham::length_ok(L) && L >= 96 && L <= 3072);
+}
+
 template <int IN>
 int dispatch_y(mm_prop* h, const void* src, int ntheta, int j, bool adj, float s, float ib, cudaStream_t st) {
     const float4* S = h->Sy + ((size_t)j * 2 + (adj ? 1 : 0)) * h->nz;
@@ -326,6 +333,12 @@ int dispatch_y(mm_prop* h, const void* src, int ntheta, int j, bool adj, float s
         case 512: return launch_y<512, IN>(h, src, ntheta, S, s, ib, st);
         case 1024: return launch_y<1024, IN>(h, src, ntheta, S, s, ib, st);
         case 2048: return launch_y<2048, IN>(h, src, ntheta, S, s, ib, st);
+        case 96: return launch_y<96, IN>(h, src, ntheta, S, s, ib, st);
+        case 192: return launch_y<192, IN>(h, src, ntheta, S, s, ib, st);
+        case 384: return launch_y<384, IN>(h, src, ntheta, S, s, ib, st);
+        case 768: return launch_y<768, IN>(h, src, ntheta, S, s, ib, st);
+        case 1536: return launch_y<1536, IN>(h, src, ntheta, S, s, ib, st);
+        case 3072: return launch_y<3072, IN>(h, src, ntheta, S, s, ib, st);
     }
     MM_REQUIRE(false, "unsupported nz=%d", h->nz);
 }
@@ -346,6 +359,12 @@ int dispatch_x(mm_prop* h, void* dst, int ntheta, int j, bool adj, cudaStream_t 
         case 512: return launch_x<512, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
         case 1024: return launch_x<1024, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
         case 2048: return launch_x<2048, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 96: return launch_x<96, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 192: return launch_x<192, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 384: return launch_x<384, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 768: return launch_x<768, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 1536: return launch_x<1536, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
+        case 3072: return launch_x<3072, OUT>(h, dst, ntheta, S, st, aux, partials, s, ib);
     }
     MM_REQUIRE(false, "unsupported n=%d", h->n);
 }
@@ -475,7 +494,7 @@ extern "C" int mm_prop_create(int n, int nz, int ntheta, int ndist, double wavel
     h->nz = nz;
     h->ntheta = ntheta;
     h->ndist = ndist;
-    h->general = !(mm_is_pow2(n) && n <= 2048 && mm_is_pow2(nz) && nz <= 2048);
+    h->general = !(native_len(n) && native_len(nz));
     std::vector<float4> sx((size_t)ndist * 2 * n), sy((size_t)ndist * 2 * nz);
     std::vector<float2> tx, ty;
     for (int j = 0; j < ndist; ++j)

@@ -28,6 +28,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 using mm::dev_alloc;
@@ -106,13 +107,20 @@ __global__ void k_transpose_out(const float2* __restrict__ B, float2* __restrict
 // scatter leaves those cells unwritten (they receive nothing), so they are
 // read as zeros.
 // ZSC: zs fixed at compile time (then the row stride (n+1)*zs is too), 0 for runtime.
+// Columns per block: four, two where four would exceed 512 threads (3 * 2^k
+// lengths, 24 values per thread).
+template <int L>
+constexpr int col_cw() {
+    return (!stockham::Sched<L>::P2 && 4 * stockham::Sched<L>::G > 512) ? 2 : 4;
+}
+
 template <int L, bool INV, int ZSC>
-__global__ void __launch_bounds__(4 * stockham::Sched<L>::G) k_col_fft(const float2* __restrict__ src,
-                                                                           float2* __restrict__ dst,
-                                                                           const float2* __restrict__ tw,
-                                                                           long ncols_rt, int zs_rt) {
+__global__ void __launch_bounds__(col_cw<L>() * stockham::Sched<L>::G) k_col_fft(const float2* __restrict__ src,
+                                                                                     float2* __restrict__ dst,
+                                                                                     const float2* __restrict__ tw,
+                                                                                     long ncols_rt, int zs_rt) {
     namespace sk = stockham;
-    constexpr int CW = 4;
+    constexpr int CW = col_cw<L>();
     const int zs = ZSC > 0 ? ZSC : zs_rt;
     const long ncols = ZSC > 0 ? (long)(L / 2 + 1) * ZSC : ncols_rt;
     extern __shared__ float2 sm[];
@@ -177,7 +185,7 @@ __global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xfwd(const TIN* _
     const int nq = min(4, zs - z0);
     // one thread per u: the four slices of one u are one 32-byte sector
     for (int k = tid; k <= n; k += 2 * G) {
-        const int km = (L - k) & (L - 1);
+        const int km = k == 0 ? 0 : L - k;
         float2 v[4];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
@@ -202,7 +210,7 @@ __global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xfwd(const TIN* _
 // u = 0 and u = n, two rows packed per complex inverse line, crop to
 // [n/2, 3n/2), times phi.  OUT 0: float obj; 1/2: real/imag part of complex.
 template <int L, int OUT, typename TOUT = float>
-__global__ void __launch_bounds__(2 * stockham::Sched<L>::G, 2) k_xinv(const float2* __restrict__ B,
+__global__ void __launch_bounds__(2 * stockham::Sched<L>::G, stockham::Sched<L>::P2 ? 2 : 1) k_xinv(const float2* __restrict__ B,
                                                                      void* __restrict__ obj,
                                                                      const float* __restrict__ phi1, float phis,
                                                                      const float2* __restrict__ tw, int nzc,
@@ -268,7 +276,7 @@ __global__ void __launch_bounds__(2 * stockham::Sched<L>::G, 2) k_xinv(const flo
 // i e^{+2 pi i k/2M} (X[k] - conj X[M-k]); x[2m] = Re z[m], x[2m+1] = Im z[m].
 // Block (G, 8): eight columns (64 bytes per k) per block.
 template <int M, typename TOUT>
-__global__ void __launch_bounds__(8 * stockham::Sched<M>::G, 2) k_rc2r(const float2* __restrict__ H,
+__global__ void __launch_bounds__(8 * stockham::Sched<M>::G, stockham::Sched<M>::P2 ? 2 : 1) k_rc2r(const float2* __restrict__ H,
                                                                      TOUT* __restrict__ out,
                                                                      const float2* __restrict__ tw,
                                                                      const float2* __restrict__ ex, long C) {
@@ -337,7 +345,7 @@ __global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rr2c(const TIN* _
     for (int idx = tid; idx < (M + 1) * CB; idx += CB * G) {
         const int c = idx & (CB - 1), k = idx >> 3;
         if (c0 + c >= C) continue;
-        const int kk = k & (M - 1), km = (M - k) & (M - 1);
+        const int kk = k == M ? 0 : k, km = k == 0 ? 0 : M - k;
         const float2 a = sm[c * LP + kk + (kk >> 4)], b = sm[c * LP + km + (km >> 4)];
         const float2 e = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));     // (Zk + conj Zm)/2
         const float2 d = make_float2(0.5f * (a.y + b.y), 0.5f * (b.x - a.x));     // (Zk - conj Zm)/(2i)
@@ -666,10 +674,11 @@ int ensure_work(mm_tomo* h, size_t need) {
 template <int L, bool INV>
 int launch_col_fft_l(mm_tomo* h, const float2* src, float2* dst, cudaStream_t st) {
     namespace sk = stockham;
-    constexpr int CW = 4, G = sk::Sched<L>::G;
+    constexpr int CW = col_cw<L>(), G = sk::Sched<L>::G;
     const long ncols = (long)(h->n + 1) * h->zs;
     const size_t smem = (size_t)sk::ColAddr<CW>::rows(L) * CW * sizeof(float2);
-    auto kern = h->zs == 64 ? k_col_fft<L, INV, 64> : k_col_fft<L, INV, 0>;
+    // 3 * 2^k lengths: runtime slice count only (one instantiation each)
+    auto kern = (sk::Sched<L>::P2 && h->zs == 64) ? k_col_fft<L, INV, sk::Sched<L>::P2 ? 64 : 0> : k_col_fft<L, INV, 0>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 block(CW, G), grid((unsigned)((ncols + CW - 1) / CW));
     kern<<<grid, block, smem, st>>>(src, dst, h->d_twy, ncols, h->zs);
@@ -694,8 +703,15 @@ int launch_col_fft(mm_tomo* h, const float2* src, float2* dst, cudaStream_t st) 
         case 1024: return launch_col_fft_l<1024, INV>(h, src, dst, st);
         case 2048: return launch_col_fft_l<2048, INV>(h, src, dst, st);
         case 4096: return launch_col_fft_l<4096, INV>(h, src, dst, st);
+        case 96: return launch_col_fft_l<96, INV>(h, src, dst, st);
+        case 192: return launch_col_fft_l<192, INV>(h, src, dst, st);
+        case 384: return launch_col_fft_l<384, INV>(h, src, dst, st);
+        case 768: return launch_col_fft_l<768, INV>(h, src, dst, st);
+        case 1536: return launch_col_fft_l<1536, INV>(h, src, dst, st);
+        case 3072: return launch_col_fft_l<3072, INV>(h, src, dst, st);
+        case 6144: return launch_col_fft_l<6144, INV>(h, src, dst, st);
     }
-    return -100;  // not a power of two in range: caller uses cuFFT
+    return -100;  // no native kernel for this length: caller uses cuFFT
 }
 
 template <int L, typename TIN>
@@ -752,6 +768,17 @@ int launch_xfwd_t(mm_tomo* h, const void* obj, int nzc, cudaStream_t st) {
         case 2048: return launch_xfwd_l<2048, TIN>(h, obj, nzc, st);
         case 4096: return launch_xfwd_l<4096, TIN>(h, obj, nzc, st);
     }
+    if constexpr (std::is_same<TIN, float>::value) {  // 3 * 2^k lengths: float32 storage only
+        switch (2 * h->n) {
+            case 96: return launch_xfwd_l<96, TIN>(h, obj, nzc, st);
+            case 192: return launch_xfwd_l<192, TIN>(h, obj, nzc, st);
+            case 384: return launch_xfwd_l<384, TIN>(h, obj, nzc, st);
+            case 768: return launch_xfwd_l<768, TIN>(h, obj, nzc, st);
+            case 1536: return launch_xfwd_l<1536, TIN>(h, obj, nzc, st);
+            case 3072: return launch_xfwd_l<3072, TIN>(h, obj, nzc, st);
+            case 6144: return launch_xfwd_l<6144, TIN>(h, obj, nzc, st);
+        }
+    }
     MM_REQUIRE(false, "x transform: unsupported n=%d", h->n);
 }
 
@@ -769,6 +796,17 @@ int launch_xinv_t(mm_tomo* h, void* obj, int nzc, cudaStream_t st) {
         case 1024: return launch_xinv_l<1024, OUT, TOUT>(h, obj, nzc, st);
         case 2048: return launch_xinv_l<2048, OUT, TOUT>(h, obj, nzc, st);
         case 4096: return launch_xinv_l<4096, OUT, TOUT>(h, obj, nzc, st);
+    }
+    if constexpr (std::is_same<TOUT, float>::value) {  // 3 * 2^k lengths: float32 storage only
+        switch (2 * h->n) {
+            case 96: return launch_xinv_l<96, OUT, TOUT>(h, obj, nzc, st);
+            case 192: return launch_xinv_l<192, OUT, TOUT>(h, obj, nzc, st);
+            case 384: return launch_xinv_l<384, OUT, TOUT>(h, obj, nzc, st);
+            case 768: return launch_xinv_l<768, OUT, TOUT>(h, obj, nzc, st);
+            case 1536: return launch_xinv_l<1536, OUT, TOUT>(h, obj, nzc, st);
+            case 3072: return launch_xinv_l<3072, OUT, TOUT>(h, obj, nzc, st);
+            case 6144: return launch_xinv_l<6144, OUT, TOUT>(h, obj, nzc, st);
+        }
     }
     MM_REQUIRE(false, "x transform: unsupported n=%d", h->n);
 }
@@ -790,6 +828,17 @@ int launch_r_t(mm_tomo* h, bool inv, const void* src, void* dst, cudaStream_t st
         case 512: return launch_r_l<512, TS>(h, inv, src, dst, st);
         case 1024: return launch_r_l<1024, TS>(h, inv, src, dst, st);
         case 2048: return launch_r_l<2048, TS>(h, inv, src, dst, st);
+    }
+    if constexpr (std::is_same<TS, float>::value) {  // 3 * 2^k lengths: float32 storage only
+        switch (h->n / 2) {
+            case 24: return launch_r_l<24, TS>(h, inv, src, dst, st);
+            case 48: return launch_r_l<48, TS>(h, inv, src, dst, st);
+            case 96: return launch_r_l<96, TS>(h, inv, src, dst, st);
+            case 192: return launch_r_l<192, TS>(h, inv, src, dst, st);
+            case 384: return launch_r_l<384, TS>(h, inv, src, dst, st);
+            case 768: return launch_r_l<768, TS>(h, inv, src, dst, st);
+            case 1536: return launch_r_l<1536, TS>(h, inv, src, dst, st);
+        }
     }
     MM_REQUIRE(false, "r transform: unsupported n=%d", h->n);
 }
@@ -931,8 +980,8 @@ extern "C" int mm_tomo_create(int n, int nz, int ntheta, const float* theta_host
     if ((rc = alloc(h, &h->d_cos, ntheta, "cos table")) || (rc = alloc(h, &h->d_sin, ntheta, "sin table")) ||
         (rc = alloc(h, &h->d_phi1, n, "phi table")))
         return fail(rc);
-    if (mm_is_pow2(2L * n) && 2 * n <= 4096) {
-        // the table of an L-point line has < 1.1 L entries; size it 2L
+    if (native_line(2L * n)) {
+        // the table of an L-point line has at most 1.5 L entries; size it 2L
         std::vector<float2> tw(4 * (size_t)n, make_float2(0.f, 0.f));
         stockham::host_twiddles(2 * n, false, tw.data());
         if ((rc = alloc(h, &h->d_twy, tw.size(), "column FFT twiddles"))) return fail(rc);
@@ -996,7 +1045,7 @@ extern "C" int mm_tomo_create(int n, int nz, int ntheta, const float* theta_host
     }
     // cuFFT plans only where no native kernel covers the size
     size_t ws = 0;
-    const bool native_col = mm_is_pow2(2L * n) && 2 * n >= 16 && 2 * n <= 4096;
+    const bool native_col = native_line(2L * n);
     if ((!h->fused_x && (rc = plan1d(&h->plan_xr2c, 2 * n, 1, 2 * n, 1, n + 1, CUFFT_R2C, (long long)zs * n, &ws))) ||
         (!native_col && (rc = plan1d(&h->plan_y, 2 * n, (long long)(n + 1) * zs, 1, (long long)(n + 1) * zs, 1,
                                      CUFFT_C2C, (long long)(n + 1) * zs, &ws))) ||
@@ -1028,7 +1077,7 @@ extern "C" int mm_tomo_R_ex(mm_tomo* h, const void* obj, int obj_dtype, void* si
     MM_REQUIRE(nz >= 1 && nz <= h->nz, "mm_tomo_R: nz=%d outside [1, %d]", nz, h->nz);
     MM_REQUIRE((obj_dtype == MM_F32 || obj_dtype == MM_BF16) && (sino_dtype == MM_F32 || sino_dtype == MM_BF16),
                "mm_tomo_R: storage dtypes must be MM_F32 or MM_BF16");
-    MM_REQUIRE((obj_dtype == MM_F32 && sino_dtype == MM_F32) || (h->fused_x && h->fused_r),
+    MM_REQUIRE((obj_dtype == MM_F32 && sino_dtype == MM_F32) || (h->fused_x && h->fused_r && mm_is_pow2(h->n)),
                "mm_tomo_R: bfloat16 storage needs n a power of two in [32, 2048]");
     MM_REQUIRE(((uintptr_t)obj % 4) == 0 && ((uintptr_t)sino % 4) == 0, "mm_tomo_R: misaligned array");
     cudaStream_t st = (cudaStream_t)stream;
@@ -1140,7 +1189,7 @@ extern "C" int mm_tomo_RT(mm_tomo* h, const void* sino, int dtype, void* obj, in
     MM_REQUIRE(h != nullptr, "mm_tomo_RT: NULL handle");
     MM_REQUIRE(sino != nullptr && obj != nullptr, "mm_tomo_RT: NULL array");
     MM_REQUIRE(dtype == MM_F32 || dtype == MM_C64 || dtype == MM_BF16, "mm_tomo_RT: dtype %d unsupported", dtype);
-    MM_REQUIRE(dtype != MM_BF16 || (h->fused_x && h->fused_r),
+    MM_REQUIRE(dtype != MM_BF16 || (h->fused_x && h->fused_r && mm_is_pow2(h->n)),
                "mm_tomo_RT: bfloat16 storage needs n a power of two in [32, 2048]");
     MM_REQUIRE(nz >= 1 && nz <= h->nz, "mm_tomo_RT: nz=%d outside [1, %d]", nz, h->nz);
     MM_REQUIRE(((uintptr_t)sino % (dtype == MM_C64 ? 8 : 4)) == 0 && ((uintptr_t)obj % 4) == 0,

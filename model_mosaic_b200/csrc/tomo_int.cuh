@@ -4,6 +4,7 @@
 #pragma once
 
 #include "mm_common.cuh"
+#include "fft_smem.cuh"
 
 #include <cuda_bf16.h>
 #include <cufft.h>
@@ -204,6 +205,12 @@ int alloc(mm_tomo* h, Tp** p, size_t count, const char* what) {
     *p = static_cast<Tp*>(q);
     h->ws_bytes += count * sizeof(Tp);
     return MM_OK;
+}
+
+// Padded line lengths 2n with native shared-memory column transforms:
+// powers of two in [16, 4096] and 3 * 2^k in [96, 6144].
+inline bool native_line(long L) {
+    return stockham::length_ok(L) && (mm_is_pow2(L) ? (L >= 16 && L <= 4096) : (L >= 96 && L <= 6144));
 }
 
 int pick_lanes(int zs, int& ZV, int& LPS) {

@@ -365,7 +365,7 @@ int launch_scatter_t(mm_tomo* h, const ScatterTable& tb, const float2* Q, float2
     // the native inverse column transform treats cells beyond radius n + 16
     // as zeros; cuFFT (other sizes) reads them, so they are written then
     const int L = 2 * h->n;
-    const int prune = (mm_is_pow2(L) && L >= 16 && L <= 4096) ? 1 : 0;
+    const int prune = native_line(L) ? 1 : 0;
     auto grid = [&](long items) {
         const long w = ((items + (32 / LPS) - 1) / (32 / LPS)) * (h->zs / (LPS * ZV));
         return (unsigned)((w * 32 + kThreads - 1) / kThreads);
