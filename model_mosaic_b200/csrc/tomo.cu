@@ -153,20 +153,34 @@ __global__ void __launch_bounds__(col_cw<L>() * stockham::Sched<L>::G) k_col_fft
 // ---------------------------------------------------------------------------
 // Fused x-side and r-side transforms (Stockham lines in shared memory).
 
+// Complex lines per x-side block: each line packs two rows (slices), so a
+// block covers 2 * x_lines() slices = one 8 * 2 * x_lines()-byte segment per
+// (v, u) of the slice-interleaved spectrum.
+template <int L>
+constexpr int x_lines() {
+    return 2;
+}
+// Blocks per SM the inverse x side is compiled for (64 registers at two).
+template <int L>
+constexpr int x_min_blocks() {
+    return (stockham::Sched<L>::P2 && x_lines<L>() * stockham::Sched<L>::G <= 512) ? 2 : 1;
+}
+
 // R x-side: rows (z, y) of phi*obj, zero padded to L = 2n, real FFT with two
 // rows packed per complex line, written slice-interleaved into the centre
-// rows of Y[v][u][z] (four slices = one 32-byte sector per u).
-// Block (G, 2): line l holds rows z0 + 2l (real part) and z0 + 2l + 1 (imag).
+// rows of Y[v][u][z] (2 NL slices = one 16 NL-byte segment per u).
+// Block (G, NL): line l holds rows z0 + 2l (real part) and z0 + 2l + 1 (imag).
 template <int L, typename TIN>
-__global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xfwd(const TIN* __restrict__ obj,
-                                                                     float2* __restrict__ Y,
-                                                                     const float* __restrict__ phi1, float phis,
-                                                                     const float2* __restrict__ tw, int nzc,
-                                                                     int zs) {
-    constexpr int n = L / 2, LP = L + L / 16, G = stockham::Sched<L>::G;
+__global__ void __launch_bounds__(x_lines<L>() * stockham::Sched<L>::G) k_xfwd(const TIN* __restrict__ obj,
+                                                                                float2* __restrict__ Y,
+                                                                                const float* __restrict__ phi1,
+                                                                                float phis,
+                                                                                const float2* __restrict__ tw,
+                                                                                int nzc, int zs) {
+    constexpr int n = L / 2, LP = L + L / 16, G = stockham::Sched<L>::G, NL = x_lines<L>(), ZB = 2 * NL;
     extern __shared__ float2 sm[];
     const int g = threadIdx.x, l = threadIdx.y;
-    const int y = blockIdx.y, z0 = blockIdx.x * 4;  // z-groups fastest: a (v, u) segment fills at once
+    const int y = blockIdx.y, z0 = blockIdx.x * ZB;  // z-groups fastest: a (v, u) segment fills at once
     const int za = z0 + 2 * l, zb = za + 1;
     const stockham::RowAddr ad{l * LP};
     const float py = phis * __ldg(phi1 + y);
@@ -182,13 +196,13 @@ __global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xfwd(const TIN* _
     stockham::fft<L, false>(sm, ad, ld, st, g, tw);
     __syncthreads();
     const int tid = l * G + g;
-    const int nq = min(4, zs - z0);
-    // one thread per u: the four slices of one u are one 32-byte sector
-    for (int k = tid; k <= n; k += 2 * G) {
+    const int nq = min(ZB, zs - z0);
+    // one thread per u: the slices of one u are one contiguous segment
+    for (int k = tid; k <= n; k += NL * G) {
         const int km = k == 0 ? 0 : L - k;
-        float2 v[4];
+        float2 v[ZB];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < NL; ++h) {
             const float2 zk = sm[h * LP + k + (k >> 4)];
             const float2 zm = sm[h * LP + km + (km >> 4)];
             // A = (Zk + conj Zm)/2 (real row), B = (Zk - conj Zm)/(2i) (imag row)
@@ -196,51 +210,52 @@ __global__ void __launch_bounds__(2 * stockham::Sched<L>::G) k_xfwd(const TIN* _
             v[2 * h + 1] = make_float2(0.5f * (zk.y + zm.y), 0.5f * (zm.x - zk.x));
         }
         float2* dst = Y + ((long)(y + n / 2) * (n + 1) + k) * zs + z0;
-        if (nq == 4) {
-            reinterpret_cast<float4*>(dst)[0] = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
-            reinterpret_cast<float4*>(dst)[1] = make_float4(v[2].x, v[2].y, v[3].x, v[3].y);
+        if (nq == ZB) {
+#pragma unroll
+            for (int h = 0; h < NL; ++h)
+                reinterpret_cast<float4*>(dst)[h] = make_float4(v[2 * h].x, v[2 * h].y, v[2 * h + 1].x, v[2 * h + 1].y);
         } else {
             for (int q = 0; q < nq; ++q) dst[q] = v[q];
         }
     }
 }
 
-// RT x-side: centre rows of B[v][u][z] for one y and four slices -> halve
+// RT x-side: centre rows of B[v][u][z] for one y and 2 NL slices -> halve
 // the interior columns (transpose of the x real FFT), real parts only at
 // u = 0 and u = n, two rows packed per complex inverse line, crop to
 // [n/2, 3n/2), times phi.  OUT 0: float obj; 1/2: real/imag part of complex.
 template <int L, int OUT, typename TOUT = float>
-__global__ void __launch_bounds__(2 * stockham::Sched<L>::G, stockham::Sched<L>::P2 ? 2 : 1) k_xinv(const float2* __restrict__ B,
-                                                                     void* __restrict__ obj,
-                                                                     const float* __restrict__ phi1, float phis,
-                                                                     const float2* __restrict__ tw, int nzc,
-                                                                     int zs) {
-    constexpr int n = L / 2, LP = L + L / 16, G = stockham::Sched<L>::G;
+__global__ void __launch_bounds__(x_lines<L>() * stockham::Sched<L>::G, x_min_blocks<L>())
+    k_xinv(const float2* __restrict__ B, void* __restrict__ obj, const float* __restrict__ phi1, float phis,
+           const float2* __restrict__ tw, int nzc, int zs) {
+    constexpr int n = L / 2, LP = L + L / 16, G = stockham::Sched<L>::G, NL = x_lines<L>(), ZB = 2 * NL;
     extern __shared__ float2 sm[];
     const int g = threadIdx.x, l = threadIdx.y;
-    const int y = blockIdx.y, z0 = blockIdx.x * 4;  // z-groups fastest: a (v, u) segment fills at once
+    const int y = blockIdx.y, z0 = blockIdx.x * ZB;  // z-groups fastest: a (v, u) segment fills at once
     const int tid = l * G + g;
-    const int nq = min(4, zs - z0);
-    // one thread per u: load the four slices (one 32-byte sector), line h
+    const int nq = min(ZB, zs - z0);
+    // one thread per u: load the slices (one contiguous segment), line h
     // gets Z = A + iB from rows 2h (A) and 2h + 1 (B)
-    for (int k = tid; k <= n; k += 2 * G) {
+    for (int k = tid; k <= n; k += NL * G) {
         const float2* src = B + ((long)(y + n / 2) * (n + 1) + k) * zs + z0;
-        float2 v[4];
-        if (nq == 4) {
-            const float4 a = __ldg(reinterpret_cast<const float4*>(src));
-            const float4 b = __ldg(reinterpret_cast<const float4*>(src) + 1);
-            v[0] = make_float2(a.x, a.y); v[1] = make_float2(a.z, a.w);
-            v[2] = make_float2(b.x, b.y); v[3] = make_float2(b.z, b.w);
+        float2 v[ZB];
+        if (nq == ZB) {
+#pragma unroll
+            for (int h = 0; h < NL; ++h) {
+                const float4 a = __ldg(reinterpret_cast<const float4*>(src) + h);
+                v[2 * h] = make_float2(a.x, a.y);
+                v[2 * h + 1] = make_float2(a.z, a.w);
+            }
         } else {
-            for (int q = 0; q < 4; ++q) v[q] = q < nq ? __ldg(src + q) : make_float2(0.f, 0.f);
+            for (int q = 0; q < ZB; ++q) v[q] = q < nq ? __ldg(src + q) : make_float2(0.f, 0.f);
         }
         const bool interior = k > 0 && k < n;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < ZB; ++q) {
             if (interior) { v[q].x *= 0.5f; v[q].y *= 0.5f; } else { v[q].y = 0.f; }
         }
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < NL; ++h) {
             const float2 A = v[2 * h], Bv = v[2 * h + 1];
             sm[h * LP + k + (k >> 4)] = make_float2(A.x - Bv.y, A.y + Bv.x);              // A + iB
             if (interior) {
@@ -716,11 +731,11 @@ int launch_col_fft(mm_tomo* h, const float2* src, float2* dst, cudaStream_t st) 
 
 template <int L, typename TIN>
 int launch_xfwd_l(mm_tomo* h, const void* obj, int nzc, cudaStream_t st) {
-    constexpr int G = stockham::Sched<L>::G;
-    const size_t smem = (size_t)2 * (L + L / 16) * sizeof(float2);
+    constexpr int G = stockham::Sched<L>::G, NL = x_lines<L>();
+    const size_t smem = (size_t)NL * (L + L / 16) * sizeof(float2);
     auto kern = k_xfwd<L, TIN>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 block(G, 2), grid((h->zs + 3) / 4, h->n);
+    dim3 block(G, NL), grid((h->zs + 2 * NL - 1) / (2 * NL), h->n);
     kern<<<grid, block, smem, st>>>((const TIN*)obj, h->Y, h->d_phi1, h->phi_scale, h->d_twy, nzc, h->zs);
     MM_LAUNCHED();
     return MM_OK;
@@ -728,11 +743,11 @@ int launch_xfwd_l(mm_tomo* h, const void* obj, int nzc, cudaStream_t st) {
 
 template <int L, int OUT, typename TOUT>
 int launch_xinv_l(mm_tomo* h, void* obj, int nzc, cudaStream_t st) {
-    constexpr int G = stockham::Sched<L>::G;
-    const size_t smem = (size_t)2 * (L + L / 16) * sizeof(float2);
+    constexpr int G = stockham::Sched<L>::G, NL = x_lines<L>();
+    const size_t smem = (size_t)NL * (L + L / 16) * sizeof(float2);
     auto kern = k_xinv<L, OUT, TOUT>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 block(G, 2), grid((h->zs + 3) / 4, h->n);
+    dim3 block(G, NL), grid((h->zs + 2 * NL - 1) / (2 * NL), h->n);
     kern<<<grid, block, smem, st>>>(h->Y, obj, h->d_phi1, h->phi_scale, h->d_twy, nzc, h->zs);
     MM_LAUNCHED();
     return MM_OK;
