@@ -31,13 +31,15 @@ from model_mosaic_b200.processing.tomo import TomoReal
 
 
 class _Tile:
-    def __init__(self, n, nz, theta, wavelength, voxelsize, distance, inv_norm, inv_beta, device):
+    def __init__(self, n, nz, theta, wavelength, voxelsize, distance, inv_norm, inv_beta, device,
+                 eps=1e-3, m=None):
         self.n, self.nz = int(n), int(nz)
         self.theta = np.asarray(theta).astype(np.float32)
         self.ntheta = len(self.theta)
         self.inv_norm = float(np.float32(1.0 / np.sqrt(self.n / self.ntheta))) if inv_norm is None else float(inv_norm)
         self.inv_beta = float(inv_beta)
-        self.tomo = TomoReal(self.n, self.nz, self.theta)
+        self.eps, self.m = float(eps), m
+        self.tomo = TomoReal(self.n, self.nz, self.theta, eps=self.eps, m=m)
         self.prop = Propagation(self.n, self.nz, self.ntheta, 1, wavelength, voxelsize, [float(distance)])
         f32 = dict(dtype=torch.float32, device=device)
         self.obj = torch.zeros((self.nz, self.n, self.n), **f32)
@@ -59,13 +61,32 @@ class _Tile:
 
 
 class TileBatch:
-    def __init__(self, tiles, wavelength, voxelsize, distance, *, beta_ratio=100.0, streams=4, device=None):
+    """``tiles``: dicts with n, theta and optionally nz (16), inv_norm, and the
+    USFFT accuracy pair eps / m (default the reference's eps = 1e-3, m from
+    eps).  ``params`` maps a tile size n to an (eps, m) pair for every tile of
+    that size that does not give its own (``autotune.tune_tiles`` returns one)."""
+
+    def __init__(self, tiles, wavelength, voxelsize, distance, *, beta_ratio=100.0, streams=4, device=None,
+                 params=None):
         require_cuda()
-        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        if isinstance(device, torch.device):
+            self.device = device
+        else:
+            self.device = torch.device("cuda", torch.cuda.current_device() if device is None else int(device))
+        params = params or {}
         with torch.cuda.device(self.device):
-            self.tiles = [_Tile(t["n"], t.get("nz", 16), t["theta"], wavelength, voxelsize, distance,
-                                t.get("inv_norm"), 1.0 / beta_ratio, self.device) for t in tiles]
-            self.streams = [torch.cuda.Stream(self.device) for _ in range(max(1, int(streams)))]
+            self.tiles = []
+            for t in tiles:
+                eps, m = params.get(int(t["n"]), (1e-3, None))
+                self.tiles.append(_Tile(t["n"], t.get("nz", 16), t["theta"], wavelength, voxelsize, distance,
+                                        t.get("inv_norm"), 1.0 / beta_ratio, self.device,
+                                        eps=t.get("eps", eps), m=t.get("m", m)))
+            self.set_streams(streams)
+        self.graph = None
+
+    def set_streams(self, streams: int):
+        """Worker streams the tiles are spread over (a captured graph is dropped)."""
+        self.streams = [torch.cuda.Stream(self.device) for _ in range(max(1, int(streams)))]
         self.graph = None
 
     # -- buffers -------------------------------------------------------------
