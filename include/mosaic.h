@@ -59,6 +59,20 @@ typedef struct mm_tomo_opts {
 int         mm_version(void);
 int         mm_last_error(char* buf, size_t len);  /* copies the message, returns its length */
 
+/* Caller-array checks, process-wide, off by default (also on with the
+ * environment variable MM_BOUNDS_CHECK=1).  When on, every compute call first
+ * checks each array argument: device memory of the current device (or mapped
+ * pinned host memory), and the bytes the call reads or writes lie inside one
+ * allocation (for arrays carved out of a larger allocation, inside that
+ * allocation).  A failure returns MM_EINVAL naming the argument, before
+ * anything is launched.  Costs one pointer query per array per call. */
+int         mm_set_bounds_check(int on);
+int         mm_get_bounds_check(void);
+/* The same check on one array, whatever the switch: MM_OK when [p, p + bytes)
+ * is device (or mapped pinned host) memory of the current device inside one
+ * allocation, else MM_EINVAL with the reason in mm_last_error(). */
+int         mm_check_array(const void* p, size_t bytes);
+
 /* ---- USFFT Radon pair ---------------------------------------------------
  * mm_tomo_create replaces TomoReal.__init__(n, nz, theta)
  *   (processing/tomo.py:30-88) and TomoLargeReal.__init__(n, theta, chunk_xy)

@@ -37,6 +37,11 @@ def _declare(L):
     L.mm_version.restype = i
     L.mm_last_error.argtypes = [C.c_char_p, sz]
     L.mm_last_error.restype = i
+    L.mm_set_bounds_check.argtypes = [i]
+    L.mm_set_bounds_check.restype = i
+    L.mm_get_bounds_check.restype = i
+    L.mm_check_array.argtypes = [p, sz]
+    L.mm_check_array.restype = i
     L.mm_tomo_create.argtypes = [i, i, i, p, p, C.POINTER(p)]
     L.mm_tomo_destroy.argtypes = [p]
     L.mm_tomo_R.argtypes = [p, p, p, i, p]
@@ -136,3 +141,15 @@ def read_timing(get, handle, names):
     kern = C.c_longlong()
     check(get(handle, ms, calls, k, C.byref(kern)))
     return {names[i]: (ms[i], calls[i]) for i in range(k)}, kern.value
+
+
+def set_bounds_check(on: bool = True) -> None:
+    """Process-wide caller-array checks of every compute call (off by
+    default): each array must be device memory of the current device holding
+    the bytes the call touches; a failure raises ValueError before anything
+    is launched.  Also on with the environment variable MM_BOUNDS_CHECK=1."""
+    check(lib().mm_set_bounds_check(int(bool(on))), "mm_set_bounds_check")
+
+
+def bounds_check() -> bool:
+    return bool(lib().mm_get_bounds_check())

@@ -234,6 +234,8 @@ extern "C" int mm_fbp_filter(mm_fbp* h, float* sino, long rows, const float* w, 
     MM_REQUIRE(rows >= 0, "mm_fbp_filter: rows=%ld negative", rows);
     MM_REQUIRE(((uintptr_t)sino % 4) == 0 && ((uintptr_t)w % 4) == 0, "mm_fbp_filter: misaligned array");
     if (rows == 0) return MM_OK;
+    MM_RANGE(sino, (size_t)rows * h->n * 4, "mm_fbp_filter", "sino");
+    MM_RANGE(w, (size_t)(h->ne / 2 + 1) * 4, "mm_fbp_filter", "w");
     cudaStream_t st = (cudaStream_t)stream;
     return h->native ? dispatch_native(h, sino, rows, w, st) : run_general(h, sino, rows, w, st);
 }

@@ -82,7 +82,21 @@ const char* cufft_name(cufftResult r);
 // dev_alloc() in this process reports MM_ENOMEM without calling cudaMalloc.
 int dev_alloc(void** p, size_t bytes, const char* what);
 
+// Caller-array checks (off by default; mm_set_bounds_check(1) or the
+// environment variable MM_BOUNDS_CHECK=1 turn them on).  When on, every
+// compute entry point checks each array it is given before it launches
+// anything: [p, p + bytes) must be device memory of the current device (or
+// mapped pinned host memory) and lie inside one allocation.  A failed check
+// returns MM_EINVAL and names the argument, so a short buffer is reported
+// instead of being written past.  Sub-allocators that carve arrays out of
+// larger cudaMalloc blocks (torch's caching allocator) are checked against
+// the block.
+bool bounds_check_on();
+int check_range(const void* p, size_t bytes, const char* who, const char* what);
+
 }  // namespace mm
+
+#define MM_RANGE(p, bytes, who, what) MM_TRY(mm::check_range((p), (bytes), (who), (what)))
 
 #define MM_CUDA(call)                                                              \
     do {                                                                           \

@@ -303,6 +303,8 @@ extern "C" int mm_pgn_retrieve(mm_pgn* h, const float* intensity, float* phase, 
     MM_REQUIRE(intensity != nullptr && phase != nullptr, "mm_pgn_retrieve: NULL array");
     MM_REQUIRE(frames >= 1 && frames <= h->ntheta, "mm_pgn_retrieve: batch %d > cached ntheta %d", frames,
                h->ntheta);
+    MM_RANGE(intensity, (size_t)frames * h->nz * h->n * 4, "mm_pgn_retrieve", "intensity");
+    MM_RANGE(phase, (size_t)frames * h->nz * h->n * 4, "mm_pgn_retrieve", "phase");
     cudaStream_t st = (cudaStream_t)stream;
     if (!h->native) return run_general(h, intensity, phase, frames, st);
     const long rows = (long)frames * h->nz;

@@ -424,11 +424,16 @@ int run_general(mm_prop* h, const void* src, void* dst, int nt, int j, bool adj,
     return MM_OK;
 }
 
-int check_call(const mm_prop* h, const void* a, const void* b, int ntheta, int j, const char* who) {
+// asz / bsz: bytes per pixel of the input a and the output b (range checks).
+int check_call(const mm_prop* h, const void* a, const void* b, int ntheta, int j, const char* who, int asz = 8,
+               int bsz = 8) {
     MM_REQUIRE(h != nullptr, "%s: NULL handle", who);
     MM_REQUIRE(a != nullptr && b != nullptr, "%s: NULL array", who);
     MM_REQUIRE(ntheta >= 1 && ntheta <= h->ntheta, "%s: ntheta=%d outside [1, %d]", who, ntheta, h->ntheta);
     MM_REQUIRE(j >= 0 && j < h->ndist, "%s: distance index %d outside [0, %d)", who, j, h->ndist);
+    const size_t px = (size_t)ntheta * h->nz * h->n;
+    MM_RANGE(a, px * asz, who, "input");
+    MM_RANGE(b, px * bsz, who, "output");
     return MM_OK;
 }
 
@@ -564,7 +569,7 @@ extern "C" int mm_prop_DT(mm_prop* h, const void* g, void* out, int ntheta, int 
 
 extern "C" int mm_prop_intensity(mm_prop* h, const float* proj, float inv_norm, float inv_beta_ratio,
                                  float* intensity, int ntheta, int j, void* stream) {
-    MM_TRY(check_call(h, proj, intensity, ntheta, j, "mm_prop_intensity"));
+    MM_TRY(check_call(h, proj, intensity, ntheta, j, "mm_prop_intensity", 4, 4));
     cudaStream_t st = (cudaStream_t)stream;
     if (h->general)
         return run_general<1, 1>(h, proj, intensity, ntheta, j, false, st, nullptr, nullptr, inv_norm, inv_beta_ratio);
@@ -706,6 +711,8 @@ extern "C" int mm_prop_D_noalloc(int n, int nz, int ntheta, double wavelength, d
                "mm_prop_D_noalloc: ntheta*nz*n=%zu needs %zu bytes of scratch, more than the %zu-byte "
                "static buffer (use mm_prop_D, or fewer angles per call)",
                (size_t)ntheta * nz * n, need, kNoAllocBytes);
+    MM_RANGE(psi, (size_t)ntheta * nz * n * 8, "mm_prop_D_noalloc", "psi");
+    MM_RANGE(out, (size_t)ntheta * nz * n * 8, "mm_prop_D_noalloc", "out");
     float2* base = nullptr;
     MM_TRY(noalloc_setup(&base));
     cudaStream_t st = (cudaStream_t)stream;
@@ -730,7 +737,11 @@ extern "C" int mm_prop_D_noalloc(int n, int nz, int ntheta, double wavelength, d
 extern "C" long mm_prop_grad_partials(mm_prop* h, int ntheta) {
     if (!h || ntheta < 1) return 0;
     if (h->general) return (long)ntheta * h->nz;
-    const int G = h->n >= 16 ? h->n / 16 : 1;
+    // threads per row line of the x-pass (stockham::Sched<n>::G): 16 values
+    // per thread for 2^k, 24 for 3 * 2^k; rows per block as x_rows()
+    const bool p2 = mm_is_pow2(h->n);
+    const int V = p2 ? 16 : 24;
+    const int G = h->n >= V ? h->n / V : 1;
     const int rpb = G >= 256 ? 1 : 256 / G;
     return ((long)ntheta * h->nz + rpb - 1) / rpb;
 }
@@ -738,8 +749,10 @@ extern "C" long mm_prop_grad_partials(mm_prop* h, int ntheta) {
 extern "C" int mm_prop_grad_forward(mm_prop* h, const float* proj, const float* data, float inv_norm,
                                     float inv_beta_ratio, void* gu, float* partials, int ntheta, int j,
                                     void* stream) {
-    MM_TRY(check_call(h, proj, gu, ntheta, j, "mm_prop_grad_forward"));
+    MM_TRY(check_call(h, proj, gu, ntheta, j, "mm_prop_grad_forward", 4, 8));
     MM_REQUIRE(data != nullptr && partials != nullptr, "mm_prop_grad_forward: NULL data/partials");
+    MM_RANGE(data, (size_t)ntheta * h->nz * h->n * 4, "mm_prop_grad_forward", "data");
+    MM_RANGE(partials, (size_t)mm_prop_grad_partials(h, ntheta) * 4, "mm_prop_grad_forward", "partials");
     cudaStream_t st = (cudaStream_t)stream;
     if (h->general)
         return run_general<1, 2>(h, proj, gu, ntheta, j, false, st, data, partials, inv_norm, inv_beta_ratio);
@@ -749,8 +762,9 @@ extern "C" int mm_prop_grad_forward(mm_prop* h, const float* proj, const float* 
 
 extern "C" int mm_prop_grad_backward(mm_prop* h, const void* gu, const float* proj, float inv_norm,
                                      float inv_beta_ratio, float* gp, int ntheta, int j, void* stream) {
-    MM_TRY(check_call(h, gu, gp, ntheta, j, "mm_prop_grad_backward"));
+    MM_TRY(check_call(h, gu, gp, ntheta, j, "mm_prop_grad_backward", 8, 4));
     MM_REQUIRE(proj != nullptr, "mm_prop_grad_backward: NULL proj");
+    MM_RANGE(proj, (size_t)ntheta * h->nz * h->n * 4, "mm_prop_grad_backward", "proj");
     cudaStream_t st = (cudaStream_t)stream;
     if (h->general)
         return run_general<0, 3>(h, gu, gp, ntheta, j, true, st, proj, nullptr, inv_norm, inv_beta_ratio);

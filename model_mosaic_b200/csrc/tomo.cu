@@ -1095,6 +1095,8 @@ extern "C" int mm_tomo_R_ex(mm_tomo* h, const void* obj, int obj_dtype, void* si
     MM_REQUIRE((obj_dtype == MM_F32 && sino_dtype == MM_F32) || (h->fused_x && h->fused_r && mm_is_pow2(h->n)),
                "mm_tomo_R: bfloat16 storage needs n a power of two in [32, 2048]");
     MM_REQUIRE(((uintptr_t)obj % 4) == 0 && ((uintptr_t)sino % 4) == 0, "mm_tomo_R: misaligned array");
+    MM_RANGE(obj, (size_t)nz * h->n * h->n * (obj_dtype == MM_BF16 ? 2 : 4), "mm_tomo_R", "obj");
+    MM_RANGE(sino, (size_t)h->ntheta * nz * h->n * (sino_dtype == MM_BF16 ? 2 : 4), "mm_tomo_R", "sino");
     cudaStream_t st = (cudaStream_t)stream;
     const int n = h->n, zs = h->zs, T = h->ntheta;
     h->tm.begin(0, st);
@@ -1209,6 +1211,11 @@ extern "C" int mm_tomo_RT(mm_tomo* h, const void* sino, int dtype, void* obj, in
     MM_REQUIRE(nz >= 1 && nz <= h->nz, "mm_tomo_RT: nz=%d outside [1, %d]", nz, h->nz);
     MM_REQUIRE(((uintptr_t)sino % (dtype == MM_C64 ? 8 : 4)) == 0 && ((uintptr_t)obj % 4) == 0,
                "mm_tomo_RT: misaligned array");
+    {
+        const size_t esz = dtype == MM_C64 ? 8 : (dtype == MM_BF16 ? 2 : 4);
+        MM_RANGE(sino, (size_t)h->ntheta * nz * h->n * esz, "mm_tomo_RT", "sino");
+        MM_RANGE(obj, (size_t)nz * h->n * h->n * esz, "mm_tomo_RT", "obj");
+    }
     cudaStream_t st = (cudaStream_t)stream;
     MM_TRY(ensure_rt(h, st));
     const int n = h->n, zs = h->zs, T = h->ntheta;

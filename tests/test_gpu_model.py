@@ -90,12 +90,15 @@ def test_autograd_function(case):
     assert torch.allclose(dl.grad, 2.0 * g, rtol=1e-6, atol=0)
 
 
-def test_general_sizes_gradient():
-    # n = 48, nz = 24: the Radon pair on its cuFFT path and D on the general
-    # (non-power-of-two) path, fused gradient against the FP64 oracle
+@pytest.mark.parametrize("n,nz,T", [(48, 24, 30), (96, 96, 36), (192, 48, 40)])
+def test_general_sizes_gradient(n, nz, T):
+    # n = 48, nz = 24: the Radon pair on the native 3 * 2^k kernels (2n = 96)
+    # and D on the general (cuFFT) path; 96^3: every stage on the native
+    # 3 * 2^k kernels (the row pass's per-block loss partials included);
+    # 192 x 48: 3 * 2^k rows and columns of D.  Fused gradient against the
+    # FP64 oracle
     from model_mosaic_b200.model import ForwardModel
     from model_mosaic_b200.phantom import ellipsoid_volume
-    n, nz, T = 48, 24, 30
     theta = np.linspace(0, np.pi, T, endpoint=False).astype(np.float32)
     delta = ellipsoid_volume(n, nz, seed=0, vmin=0.2, vmax=1.0)
     delta2 = ellipsoid_volume(n, nz, seed=1, vmin=0.2, vmax=1.0)
@@ -107,6 +110,11 @@ def test_general_sizes_gradient():
     d32 = torch.from_numpy(d.astype(np.float32)).cuda()
     loss, g = m.loss_and_grad(dl, d32)
     assert abs(float(loss) - ora.loss(delta, d)) / ora.loss(delta, d) < 1e-5
-    assert rl2(g.cpu().numpy(), ora.grad(delta, d)) < 1e-5
+    # the gradient ends in RT of a noise-like adjoint sinogram, whose float32
+    # sums have an error floor of their own (the same composition in float32:
+    # 2.3e-5 at 192 x 48, 40 angles): gate max(1e-5, 1.5 x that floor)
+    g64 = ora.grad(delta, d)
+    floor = rl2(ModelOracle(n, nz, theta, WL, VOX, DIST, s=s, dtype=np.float32).grad(delta, d), g64)
+    assert rl2(g.cpu().numpy(), g64) < max(1e-5, 1.5 * floor)
     l2, g2 = m.plain_loss_and_grad(dl, d32)
     assert rl2(g.cpu().numpy(), g2.cpu().numpy()) < 1e-6
