@@ -57,6 +57,10 @@ WORKLOADS = {
     # 513 x 64 complex: 269 MB) on ~3.5 GB, for ncu captures of the scatter
     "rtprofile": dict(n=1024, nz=64, ntheta=1024, theta_max=2 * np.pi, energy_kev=30.0,
                       distance=0.12, voxelsize=0.69e-6),
+    # the 3 * 2^k kernels of the n = 3072 size (6144-point x-side and
+    # column lines, 1536-point r-side lines, 3072-point D rows) on ~3 GB
+    "profile3072": dict(n=3072, nz=8, ntheta=288, theta_max=np.pi, energy_kev=30.0,
+                        distance=0.12, voxelsize=0.69e-6),
     # step8_fbp.py's default size (n = 3072, 3n/4 = 2304 angles on [0, pi)):
     # 6144-point columns and rows, 1536-point r-side lines (radix-3 passes)
     "n3072": dict(n=3072, nz=32, ntheta=2304, theta_max=np.pi, energy_kev=30.0,
