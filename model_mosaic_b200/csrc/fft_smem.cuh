@@ -19,6 +19,8 @@ namespace mmfft {
 // W_64^j = exp(-2*pi*i*j/64).  Each translation unit that includes this
 // header owns a copy; init_constants() uploads it once per device.
 static __constant__ float2 c_w64[64];
+// W_48^j, for the twiddles of the 24-point register FFT (3 x 8).
+static __constant__ float2 c_w48[48];
 
 static inline cudaError_t init_constants() {
     static bool done[64] = {false};
@@ -32,6 +34,13 @@ static inline cudaError_t init_constants() {
         w[j] = make_float2((float)cos(a), (float)sin(a));
     }
     e = cudaMemcpyToSymbol(c_w64, w, sizeof(w));
+    if (e != cudaSuccess) return e;
+    float2 w48[48];
+    for (int j = 0; j < 48; ++j) {
+        const double a = -2.0 * 3.14159265358979323846 * j / 48.0;
+        w48[j] = make_float2((float)cos(a), (float)sin(a));
+    }
+    e = cudaMemcpyToSymbol(c_w48, w48, sizeof(w48));
     if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
     return e;
 }
@@ -123,7 +132,15 @@ __device__ __forceinline__ void reg_fft3(float2 (&v)[R]) {
         float2 y1 = make_float2(m.x + sh * d.y, m.y - sh * d.x);
         float2 y2 = make_float2(m.x - sh * d.y, m.y + sh * d.x);
         if (n2 > 0) {
-            const float2 w1 = w12(n2 * (12 / R)), w2 = w12(2 * n2 * (12 / R));
+            float2 w1, w2;
+            if constexpr (12 % R == 0) {  // R = 3, 6, 12: compile-time constants
+                w1 = w12(n2 * (12 / R));
+                w2 = w12(2 * n2 * (12 / R));
+            } else {                      // R = 24: the W_48 table
+                static_assert(48 % R == 0, "3 * 2^a register FFTs up to 24 points");
+                w1 = c_w48[(n2 * (48 / R)) % 48];
+                w2 = c_w48[(2 * n2 * (48 / R)) % 48];
+            }
             y1 = INV ? cmulc(y1, w1) : cmul(y1, w1);
             y2 = INV ? cmulc(y2, w2) : cmul(y2, w2);
         }
@@ -138,7 +155,7 @@ __device__ __forceinline__ void reg_fft3(float2 (&v)[R]) {
     }
 }
 
-// In-register FFT of size R (a power of two <= 64, or 3, 6, 12), natural
+// In-register FFT of size R (a power of two <= 64, or 3, 6, 12, 24), natural
 // order in and out.  INV = false: exp(-2 pi i ...); INV = true:
 // exp(+2 pi i ...), unnormalised.
 template <int R, bool INV>
@@ -206,17 +223,22 @@ __host__ __device__ constexpr bool length_ok(long L) {
 // inverse half of a convolution uses the reversed schedule so that its first
 // pass owns exactly the elements the forward's last pass produced (see
 // conv()).
-template <int L, bool REV = false>
+// VW = 48 selects the wide form of a 3 * 2^k line (L >= 48): base radix 16
+// and 48 values per thread, the last pass of radix 3, 6, 12 or 24 -- half the
+// threads per line, for kernels that want more lines per block.
+template <int L, bool REV = false, int VW = 0>
 struct Sched {
     static_assert(length_ok(L), "line length must be 2^k or 3 * 2^k");
     static constexpr bool P2 = (L & (L - 1)) == 0;
-    static constexpr int B = P2 ? 16 : 8;                         // base radix
-    static constexpr int VB = P2 ? 16 : 24;                       // values per thread
+    static_assert(VW == 0 || (VW == 48 && !P2 && L >= 48), "wide schedule: 3 * 2^k lines of 48 or more");
+    static constexpr bool W = VW == 48;
+    static constexpr int B = (P2 || W) ? 16 : 8;                  // base radix
+    static constexpr int VB = P2 ? 16 : (W ? 48 : 24);            // values per thread
     static constexpr int K2 = ilog2<P2 ? L : L / 3>();            // exponent of the power-of-two factor
-    static constexpr int P = P2 ? (L <= 16 ? 1 : (K2 + 3) / 4) : 1 + K2 / 3;   // passes
+    static constexpr int P = P2 ? (L <= 16 ? 1 : (K2 + 3) / 4) : (W ? 1 + K2 / 4 : 1 + K2 / 3);   // passes
     static constexpr int G = L >= VB ? L / VB : 1;                // threads per line
     static constexpr int V = L >= VB ? VB : L;                    // values per thread
-    static constexpr int small = P2 ? (L >> (4 * (P - 1))) : (L >> (3 * (P - 1)));
+    static constexpr int small = (P2 || W) ? (L >> (4 * (P - 1))) : (L >> (3 * (P - 1)));
     static constexpr int radix(int p) { return REV ? (p == 0 ? small : B) : (p < P - 1 ? B : small); }
     static constexpr int span(int p) {
         int s = 1;
@@ -231,17 +253,18 @@ struct Sched {
     static constexpr int tw_size() { return tw_off(P); }
 };
 
-// Host-side table for Sched<L, rev> (FP64 angles), Sched<L, rev>::tw_size()
+// Host-side table for Sched<L, rev, wide ? 48 : 0> (FP64 angles), its tw_size()
 // entries: pass p >= 1, W_{NS*RP}^(i*k) at [off_p + i*NS + k].  Returns the
 // entry count (at most 1.5 L), or -1 for a length the engine does not cover.
-inline int host_twiddles(int L, bool rev, float2* out) {
+inline int host_twiddles(int L, bool rev, float2* out, bool wide = false) {
     if (!length_ok(L)) return -1;
     const bool p2 = (L & (L - 1)) == 0;
+    if (wide && (p2 || L < 48)) return -1;
     int k2 = 0;
     while ((1L << (k2 + 1)) <= (p2 ? L : L / 3)) ++k2;
-    const int P = p2 ? (L <= 16 ? 1 : (k2 + 3) / 4) : 1 + k2 / 3;
-    const int base = p2 ? 16 : 8;
-    const int small = p2 ? (L >> (4 * (P - 1))) : (L >> (3 * (P - 1)));
+    const int P = p2 ? (L <= 16 ? 1 : (k2 + 3) / 4) : (wide ? 1 + k2 / 4 : 1 + k2 / 3);
+    const int base = (p2 || wide) ? 16 : 8;
+    const int small = (p2 || wide) ? (L >> (4 * (P - 1))) : (L >> (3 * (P - 1)));
     auto radix = [&](int p) { return rev ? (p == 0 ? small : base) : (p < P - 1 ? base : small); };
     int o = 0, ns = radix(0);
     for (int p = 1; p < P; ++p) {
@@ -259,9 +282,9 @@ inline int host_twiddles(int L, bool rev, float2* out) {
 
 // Registers of one thread in pass PASS: groups j = t + G*q, element i of
 // group j at line position j + i*NG.
-template <int L, bool REV, int PASS>
+template <int L, bool REV, int PASS, int VW = 0>
 struct PassShape {
-    using S = Sched<L, REV>;
+    using S = Sched<L, REV, VW>;
     static constexpr int RP = S::radix(PASS);
     static constexpr int NS = S::span(PASS);
     static constexpr int NG = L / RP;
@@ -269,11 +292,12 @@ struct PassShape {
     static_assert(Q * RP == S::V, "V values per thread in every pass");
 };
 
-template <int L, bool REV, int PASS, bool INV, class Src>
-__device__ __forceinline__ void pass_load(float2 (&x)[PassShape<L, REV, PASS>::Q][PassShape<L, REV, PASS>::RP],
-                                          const Src& src, int t, const float2* __restrict__ tw) {
-    using Sh = PassShape<L, REV, PASS>;
-    using S = Sched<L, REV>;
+template <int L, bool REV, int PASS, bool INV, int VW = 0, class Src>
+__device__ __forceinline__ void pass_load(
+    float2 (&x)[PassShape<L, REV, PASS, VW>::Q][PassShape<L, REV, PASS, VW>::RP], const Src& src, int t,
+    const float2* __restrict__ tw) {
+    using Sh = PassShape<L, REV, PASS, VW>;
+    using S = Sched<L, REV, VW>;
 #pragma unroll
     for (int q = 0; q < Sh::Q; ++q) {
         const int j = t + S::G * q;
@@ -292,11 +316,11 @@ __device__ __forceinline__ void pass_load(float2 (&x)[PassShape<L, REV, PASS>::Q
     }
 }
 
-template <int L, bool REV, int PASS, class Dst>
-__device__ __forceinline__ void pass_store(float2 (&x)[PassShape<L, REV, PASS>::Q][PassShape<L, REV, PASS>::RP],
-                                           const Dst& dst, int t) {
-    using Sh = PassShape<L, REV, PASS>;
-    using S = Sched<L, REV>;
+template <int L, bool REV, int PASS, int VW = 0, class Dst>
+__device__ __forceinline__ void pass_store(
+    float2 (&x)[PassShape<L, REV, PASS, VW>::Q][PassShape<L, REV, PASS, VW>::RP], const Dst& dst, int t) {
+    using Sh = PassShape<L, REV, PASS, VW>;
+    using S = Sched<L, REV, VW>;
 #pragma unroll
     for (int q = 0; q < Sh::Q; ++q) {
         const int j = t + S::G * q;
@@ -309,32 +333,32 @@ __device__ __forceinline__ void pass_store(float2 (&x)[PassShape<L, REV, PASS>::
 
 // Passes FIRST..LAST of a transform through shared memory; pass 0 reads
 // through `ld`, pass P-1 writes through `st`, every other access is buf.
-template <int L, bool REV, bool INV, int PASS, int LAST, class Ld, class St, class Ad>
+template <int L, bool REV, bool INV, int PASS, int LAST, int VW = 0, class Ld, class St, class Ad>
 __device__ __forceinline__ void run(float2* __restrict__ buf, const Ad& ad, const Ld& ld, const St& st, int t,
                                    const float2* __restrict__ tw) {
-    using Sh = PassShape<L, REV, PASS>;
-    using S = Sched<L, REV>;
+    using Sh = PassShape<L, REV, PASS, VW>;
+    using S = Sched<L, REV, VW>;
     float2 x[Sh::Q][Sh::RP];
     auto from_buf = [&](int pos) -> float2 { return buf[ad(pos)]; };
-    if constexpr (PASS == 0) pass_load<L, REV, PASS, INV>(x, ld, t, tw);
-    else pass_load<L, REV, PASS, INV>(x, from_buf, t, tw);
+    if constexpr (PASS == 0) pass_load<L, REV, PASS, INV, VW>(x, ld, t, tw);
+    else pass_load<L, REV, PASS, INV, VW>(x, from_buf, t, tw);
     __syncthreads();  // everyone has read this pass's input
     if constexpr (PASS == S::P - 1) {
-        pass_store<L, REV, PASS>(x, st, t);
+        pass_store<L, REV, PASS, VW>(x, st, t);
     } else {
         auto to_buf = [&](int pos, float2 v) { buf[ad(pos)] = v; };
-        pass_store<L, REV, PASS>(x, to_buf, t);
+        pass_store<L, REV, PASS, VW>(x, to_buf, t);
         __syncthreads();
     }
-    if constexpr (PASS < LAST) run<L, REV, INV, PASS + 1, LAST>(buf, ad, ld, st, t, tw);
+    if constexpr (PASS < LAST) run<L, REV, INV, PASS + 1, LAST, VW>(buf, ad, ld, st, t, tw);
 }
 
 // One transform: natural order in (`ld`) and out (`st`).  Callers
-// synchronise before reusing `buf` after it returns.  tw: Sched<L, false>.
-template <int L, bool INV, class Ld, class St, class Ad>
+// synchronise before reusing `buf` after it returns.  tw: Sched<L, false, VW>.
+template <int L, bool INV, int VW = 0, class Ld, class St, class Ad>
 __device__ __forceinline__ void fft(float2* __restrict__ buf, const Ad& ad, const Ld& ld, const St& st, int t,
                                     const float2* __restrict__ tw) {
-    run<L, false, INV, 0, Sched<L>::P - 1>(buf, ad, ld, st, t, tw);
+    run<L, false, INV, 0, Sched<L, false, VW>::P - 1, VW>(buf, ad, ld, st, t, tw);
 }
 
 // Circular convolution y = IFFT(mul(k) * FFT(x)) (both unnormalised): the

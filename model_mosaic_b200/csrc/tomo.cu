@@ -107,18 +107,30 @@ __global__ void k_transpose_out(const float2* __restrict__ B, float2* __restrict
 // scatter leaves those cells unwritten (they receive nothing), so they are
 // read as zeros.
 // ZSC: zs fixed at compile time (then the row stride (n+1)*zs is too), 0 for runtime.
-// Columns per block: four, two where four would exceed 512 threads (3 * 2^k
-// lengths, 24 values per thread).
+// Schedule width of the x-side forward and column transforms: 6144-point
+// lines (n = 3072) take the wide 3 * 2^k schedule (48 values per thread), so
+// that a column block holds four columns (32-byte row segments) at 512
+// threads; measured 4.34 -> 3.85 ms forward column, 4.39 -> 4.02 ms inverse,
+// 2.06 -> 1.87 ms x side at n = 3072.  (The x-side inverse keeps the default
+// schedule: at 48 values per thread it needs 244 registers and ran slower.)
+template <int L>
+constexpr int xcol_vw() {
+    return (!stockham::Sched<L>::P2 && L >= 6144) ? 48 : 0;
+}
+template <int L>
+using ColSched = stockham::Sched<L, false, xcol_vw<L>()>;
+
+// Columns per block: four, two where four would exceed 512 threads.
 template <int L>
 constexpr int col_cw() {
-    return (!stockham::Sched<L>::P2 && 4 * stockham::Sched<L>::G > 512) ? 2 : 4;
+    return (!ColSched<L>::P2 && 4 * ColSched<L>::G > 512) ? 2 : 4;
 }
 
 template <int L, bool INV, int ZSC>
-__global__ void __launch_bounds__(col_cw<L>() * stockham::Sched<L>::G) k_col_fft(const float2* __restrict__ src,
-                                                                                     float2* __restrict__ dst,
-                                                                                     const float2* __restrict__ tw,
-                                                                                     long ncols_rt, int zs_rt) {
+__global__ void __launch_bounds__(col_cw<L>() * ColSched<L>::G) k_col_fft(const float2* __restrict__ src,
+                                                                              float2* __restrict__ dst,
+                                                                              const float2* __restrict__ tw,
+                                                                              long ncols_rt, int zs_rt) {
     namespace sk = stockham;
     constexpr int CW = col_cw<L>();
     const int zs = ZSC > 0 ? ZSC : zs_rt;
@@ -147,7 +159,7 @@ __global__ void __launch_bounds__(col_cw<L>() * stockham::Sched<L>::G) k_col_fft
         }
         if (live) dst[(long)pos * ncols + col] = v;
     };
-    sk::fft<L, INV>(sm, ad, ld, st, g, tw);
+    sk::fft<L, INV, xcol_vw<L>()>(sm, ad, ld, st, g, tw);
 }
 
 // ---------------------------------------------------------------------------
@@ -171,13 +183,13 @@ constexpr int x_min_blocks() {
 // rows of Y[v][u][z] (2 NL slices = one 16 NL-byte segment per u).
 // Block (G, NL): line l holds rows z0 + 2l (real part) and z0 + 2l + 1 (imag).
 template <int L, typename TIN>
-__global__ void __launch_bounds__(x_lines<L>() * stockham::Sched<L>::G) k_xfwd(const TIN* __restrict__ obj,
+__global__ void __launch_bounds__(x_lines<L>() * ColSched<L>::G) k_xfwd(const TIN* __restrict__ obj,
                                                                                 float2* __restrict__ Y,
                                                                                 const float* __restrict__ phi1,
                                                                                 float phis,
                                                                                 const float2* __restrict__ tw,
                                                                                 int nzc, int zs) {
-    constexpr int n = L / 2, LP = L + L / 16, G = stockham::Sched<L>::G, NL = x_lines<L>(), ZB = 2 * NL;
+    constexpr int n = L / 2, LP = L + L / 16, G = ColSched<L>::G, NL = x_lines<L>(), ZB = 2 * NL;
     extern __shared__ float2 sm[];
     const int g = threadIdx.x, l = threadIdx.y;
     const int y = blockIdx.y, z0 = blockIdx.x * ZB;  // z-groups fastest: a (v, u) segment fills at once
@@ -193,7 +205,7 @@ __global__ void __launch_bounds__(x_lines<L>() * stockham::Sched<L>::G) k_xfwd(c
         return make_float2(za < nzc ? w * ld_elem(ra + x) : 0.f, zb < nzc ? w * ld_elem(rb + x) : 0.f);
     };
     auto st = [&](int pos, float2 v) { sm[ad(pos)] = v; };
-    stockham::fft<L, false>(sm, ad, ld, st, g, tw);
+    stockham::fft<L, false, xcol_vw<L>()>(sm, ad, ld, st, g, tw);
     __syncthreads();
     const int tid = l * G + g;
     const int nq = min(ZB, zs - z0);
@@ -689,14 +701,14 @@ int ensure_work(mm_tomo* h, size_t need) {
 template <int L, bool INV>
 int launch_col_fft_l(mm_tomo* h, const float2* src, float2* dst, cudaStream_t st) {
     namespace sk = stockham;
-    constexpr int CW = col_cw<L>(), G = sk::Sched<L>::G;
+    constexpr int CW = col_cw<L>(), G = ColSched<L>::G;
     const long ncols = (long)(h->n + 1) * h->zs;
     const size_t smem = (size_t)sk::ColAddr<CW>::rows(L) * CW * sizeof(float2);
     // 3 * 2^k lengths: runtime slice count only (one instantiation each)
     auto kern = (sk::Sched<L>::P2 && h->zs == 64) ? k_col_fft<L, INV, sk::Sched<L>::P2 ? 64 : 0> : k_col_fft<L, INV, 0>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 block(CW, G), grid((unsigned)((ncols + CW - 1) / CW));
-    kern<<<grid, block, smem, st>>>(src, dst, h->d_twy, ncols, h->zs);
+    kern<<<grid, block, smem, st>>>(src, dst, xcol_vw<L>() ? h->d_tww : h->d_twy, ncols, h->zs);
     MM_LAUNCHED();
     return MM_OK;
 }
@@ -731,12 +743,13 @@ int launch_col_fft(mm_tomo* h, const float2* src, float2* dst, cudaStream_t st) 
 
 template <int L, typename TIN>
 int launch_xfwd_l(mm_tomo* h, const void* obj, int nzc, cudaStream_t st) {
-    constexpr int G = stockham::Sched<L>::G, NL = x_lines<L>();
+    constexpr int G = ColSched<L>::G, NL = x_lines<L>();
     const size_t smem = (size_t)NL * (L + L / 16) * sizeof(float2);
     auto kern = k_xfwd<L, TIN>;
     MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 block(G, NL), grid((h->zs + 2 * NL - 1) / (2 * NL), h->n);
-    kern<<<grid, block, smem, st>>>((const TIN*)obj, h->Y, h->d_phi1, h->phi_scale, h->d_twy, nzc, h->zs);
+    kern<<<grid, block, smem, st>>>((const TIN*)obj, h->Y, h->d_phi1, h->phi_scale,
+                                    xcol_vw<L>() ? h->d_tww : h->d_twy, nzc, h->zs);
     MM_LAUNCHED();
     return MM_OK;
 }
@@ -926,7 +939,7 @@ void destroy(mm_tomo* h) {
     cufftHandle all[6] = {h->plan_xr2c, h->plan_xc2r, h->plan_y, h->plan_rc2r, h->plan_rr2c, h->plan_rc2c};
     for (cufftHandle p : all)
         if (p) cufftDestroy(p);
-    void* bufs[] = {h->d_cos, h->d_sin, h->d_phi1, h->d_twy, h->d_twr, h->d_exr, h->col_scratch, h->col_tw, h->P, h->X, h->Y, h->F, h->Hh, h->sino_tmp, h->fft_work,
+    void* bufs[] = {h->d_cos, h->d_sin, h->d_phi1, h->d_twy, h->d_tww, h->d_twr, h->d_exr, h->col_scratch, h->col_tw, h->P, h->X, h->Y, h->F, h->Hh, h->sino_tmp, h->fft_work,
                     h->ypad, h->yc};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -1003,6 +1016,16 @@ extern "C" int mm_tomo_create(int n, int nz, int ntheta, const float* theta_host
         if (cudaMemcpy(h->d_twy, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess) {
             mm::set_error("mm_tomo_create: table upload failed");
             return fail(MM_ECUDA);
+        }
+        if (!mm_is_pow2(2L * n) && 2 * n >= 6144) {  // the wide schedule of the x-side forward and columns
+            std::vector<float2> tww(4 * (size_t)n, make_float2(0.f, 0.f));
+            stockham::host_twiddles(2 * n, false, tww.data(), true);
+            if ((rc = alloc(h, &h->d_tww, tww.size(), "wide column FFT twiddles"))) return fail(rc);
+            if (cudaMemcpy(h->d_tww, tww.data(), tww.size() * sizeof(float2), cudaMemcpyHostToDevice) !=
+                cudaSuccess) {
+                mm::set_error("mm_tomo_create: table upload failed");
+                return fail(MM_ECUDA);
+            }
         }
         h->fused_x = 2 * n >= 64;
         const int M = n / 2;

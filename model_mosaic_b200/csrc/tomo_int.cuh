@@ -37,6 +37,7 @@ struct mm_tomo {
     float* d_sin = nullptr;
     float* d_phi1 = nullptr;
     float2* d_twy = nullptr;     // Stockham twiddles of the 2n-point x and column transforms
+    float2* d_tww = nullptr;     // the same for the wide 3 * 2^k schedule (2n >= 6144)
     float2* d_twr = nullptr;     // Stockham twiddles of the n/2-point r transforms
     float2* d_exr = nullptr;     // e^{+2 pi i k/n}, k = 0..n/2 (real-from-half-length packing)
     float2* col_scratch = nullptr;  // L2-resident per-SM regions of the 64 x 64 column transform

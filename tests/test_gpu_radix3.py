@@ -107,3 +107,59 @@ def test_paganin_vs_fp64(n, nz, nt):
     p = Paganin(n, nz, nt, wl, vox, 0.1, alpha)
     ref = retrieve(x, paganin_filter(n, nz, wl, vox, 0.1, alpha))
     assert rl2(p.retrieve(x), ref) < RTOL
+
+
+@pytest.mark.parametrize("n,nz", [(96, 3), (384, 1)])
+def test_paired_360_and_complex_rt(n, nz):
+    # 360-degree scans take the paired (theta, theta + pi) gather; complex RT input
+    from model_mosaic_b200.phantom import ellipsoid_volume
+    from model_mosaic_b200.processing.tomo import TomoReal
+    T = 3 * n // 2
+    theta = np.linspace(0, 2 * np.pi, T, endpoint=False).astype(np.float32)
+    x = ellipsoid_volume(n, nz, seed=n + 7, count=10)
+    tomo = TomoReal(n, nz, theta)
+    o = TomoRealOracle(n, nz, theta)
+    assert rl2(tomo.R(x), o.R(x)) < RTOL
+    rng = np.random.default_rng(n)
+    yp = o.R(ellipsoid_volume(n, nz, seed=n + 8, count=10))
+    yc = (yp + 1j * o.R(ellipsoid_volume(n, nz, seed=n + 9, count=10))).astype(np.complex64)
+    rec = tomo.RT(yc)
+    assert rec.dtype == np.complex64
+    assert rl2(rec, o.RT(yc)) < RTOL
+
+
+def test_large_classes_at_3x2k():
+    from model_mosaic_b200.phantom import ellipsoid_volume
+    from model_mosaic_b200.processing.propagation import Propagation
+    from model_mosaic_b200.processing.propagation_large import PropagationLarge
+    from model_mosaic_b200.processing.tomo import TomoReal
+    from model_mosaic_b200.processing.tomo_large import TomoLargeReal
+    n, nz, T = 192, 5, 144
+    theta = np.linspace(0, np.pi, T, endpoint=False).astype(np.float32)
+    x = ellipsoid_volume(n, nz, seed=3, count=10)
+    tl = TomoLargeReal(n, theta, 64)
+    s = tl.R(x, [64, 48, 64]).copy()
+    tr = TomoReal(n, nz, theta, clamp_xy=True)
+    assert rl2(s, tr.R(x)) < 1e-6                      # the Large class runs the same kernels
+    assert rl2(s, TomoRealOracle(n, nz, theta).R(x, clamp=True)) < RTOL
+    assert rl2(tl.RT(s, [64, 48, 64]), tr.RT(s)) < 1e-6
+    wl, vs = 4.133e-11, 0.69e-6
+    psi = (np.random.default_rng(1).standard_normal((3, 96, 384))
+           + 1j * np.random.default_rng(2).standard_normal((3, 96, 384))).astype(np.complex64)
+    pl = PropagationLarge(384, 96, wl, vs, [0.12])
+    pg = Propagation(384, 96, 3, 1, wl, vs, [0.12])
+    ref = PropagationOracle(384, 96, 3, 1, wl, vs, [0.12]).D(psi, 0)
+    assert rl2(pl.D(psi, 0, [48, 192]), ref) < RTOL
+    assert rl2(pg.D(psi, 0), ref) < RTOL
+
+
+@pytest.mark.parametrize("n,nz,nt", [(384, 96, 3), (192, 3072, 1)])
+def test_intensity_fused_stage_3x2k(n, nz, nt):
+    from oracle.fresnel import abs2, psi_from_proj
+    from model_mosaic_b200.processing.propagation import Propagation
+    wl, vs = 4.133e-11, 0.69e-6
+    p = np.random.default_rng(5).uniform(0, 3, (nt, nz, n)).astype(np.float32)
+    prop = Propagation(n, nz, nt, 1, wl, vs, [0.12])
+    got = prop.intensity(torch.from_numpy(p).cuda(), 0.7, 0.01, 0).cpu().numpy()
+    ref = abs2(PropagationOracle(n, nz, nt, 1, wl, vs, [0.12]).D(psi_from_proj(p, 0.7, 0.01), 0))
+    assert rl2(got, ref) < RTOL
