@@ -209,26 +209,20 @@ __global__ void __launch_bounds__(x_lines<L>() * ColSched<L>::G) k_xfwd(const TI
     __syncthreads();
     const int tid = l * G + g;
     const int nq = min(ZB, zs - z0);
-    // one thread per u: the slices of one u are one contiguous segment
-    for (int k = tid; k <= n; k += NL * G) {
+    // NL lanes per u, lane h storing line h's two slices (16 bytes): a warp
+    // store covers 32/NL whole segments instead of 32 half segments, half the
+    // L1 wavefronts of one lane per u
+    for (int idx = tid; idx < NL * (n + 1); idx += NL * G) {
+        const int k = idx / NL, h = idx % NL;
         const int km = k == 0 ? 0 : L - k;
-        float2 v[ZB];
-#pragma unroll
-        for (int h = 0; h < NL; ++h) {
-            const float2 zk = sm[h * LP + k + (k >> 4)];
-            const float2 zm = sm[h * LP + km + (km >> 4)];
-            // A = (Zk + conj Zm)/2 (real row), B = (Zk - conj Zm)/(2i) (imag row)
-            v[2 * h] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-            v[2 * h + 1] = make_float2(0.5f * (zk.y + zm.y), 0.5f * (zm.x - zk.x));
-        }
-        float2* dst = Y + ((long)(y + n / 2) * (n + 1) + k) * zs + z0;
-        if (nq == ZB) {
-#pragma unroll
-            for (int h = 0; h < NL; ++h)
-                reinterpret_cast<float4*>(dst)[h] = make_float4(v[2 * h].x, v[2 * h].y, v[2 * h + 1].x, v[2 * h + 1].y);
-        } else {
-            for (int q = 0; q < nq; ++q) dst[q] = v[q];
-        }
+        const float2 zk = sm[h * LP + k + (k >> 4)];
+        const float2 zm = sm[h * LP + km + (km >> 4)];
+        // A = (Zk + conj Zm)/2 (real row), B = (Zk - conj Zm)/(2i) (imag row)
+        const float2 A = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        const float2 Bv = make_float2(0.5f * (zk.y + zm.y), 0.5f * (zm.x - zk.x));
+        float2* dst = Y + ((long)(y + n / 2) * (n + 1) + k) * zs + z0 + 2 * h;
+        if (2 * h + 1 < nq) reinterpret_cast<float4*>(dst)[0] = make_float4(A.x, A.y, Bv.x, Bv.y);
+        else if (2 * h < nq) dst[0] = A;
     }
 }
 
@@ -247,7 +241,8 @@ __global__ void __launch_bounds__(x_lines<L>() * stockham::Sched<L>::G, x_min_bl
     const int tid = l * G + g;
     const int nq = min(ZB, zs - z0);
     // one thread per u: load the slices (one contiguous segment), line h
-    // gets Z = A + iB from rows 2h (A) and 2h + 1 (B)
+    // gets Z = A + iB from rows 2h (A) and 2h + 1 (B).  (Two lanes per u as
+    // in k_xfwd's stores measured 1.31 -> 1.32 ms here, and slower at 6144.)
     for (int k = tid; k <= n; k += NL * G) {
         const float2* src = B + ((long)(y + n / 2) * (n + 1) + k) * zs + z0;
         float2 v[ZB];
