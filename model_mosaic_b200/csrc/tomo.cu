@@ -343,16 +343,25 @@ __global__ void __launch_bounds__(8 * stockham::Sched<M>::G, stockham::Sched<M>:
     stockham::fft<M, true>(sm, ad, ld, st, g, tw);
 }
 
+// Columns (rows y[c]) per block of the RT r side.
+template <int M>
+constexpr int rr_cols() {
+    return 8;
+}
+
 // RT r-side: R2C of length 2M of real rows y[c][0..2M) as a complex forward
 // line z[m] = y[2m] + i y[2m+1]; X[k] = (Z[k] + conj Z[M-k])/2 +
 // e^{-2 pi i k/2M} (Z[k] - conj Z[M-k])/(2i) for k = 0..M, written to
-// H[k][c] (eight columns = 64 bytes per k).
+// H[k][c] (CB columns = 8 CB bytes per k).
 template <int M, typename TIN>
-__global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rr2c(const TIN* __restrict__ yv,
-                                                                     float2* __restrict__ H,
-                                                                     const float2* __restrict__ tw,
-                                                                     const float2* __restrict__ ex, long C) {
-    constexpr int CB = 8, LP = M + M / 16, G = stockham::Sched<M>::G;
+__global__ void __launch_bounds__(rr_cols<M>() * stockham::Sched<M>::G) k_rr2c(const TIN* __restrict__ yv,
+                                                                                float2* __restrict__ H,
+                                                                                const float2* __restrict__ tw,
+                                                                                const float2* __restrict__ ex,
+                                                                                long C) {
+    // odd line stride: the epilogue's CB lanes at one k read CB different
+    // lines, which then fall in different banks
+    constexpr int CB = rr_cols<M>(), LP = M + M / 16 + 1, G = stockham::Sched<M>::G;
     extern __shared__ float2 sm[];
     const int g = threadIdx.x, l = threadIdx.y;
     const long c0 = (long)blockIdx.x * CB;
@@ -365,7 +374,7 @@ __global__ void __launch_bounds__(8 * stockham::Sched<M>::G) k_rr2c(const TIN* _
     __syncthreads();
     const int tid = l * G + g;
     for (int idx = tid; idx < (M + 1) * CB; idx += CB * G) {
-        const int c = idx & (CB - 1), k = idx >> 3;
+        const int c = idx % CB, k = idx / CB;
         if (c0 + c >= C) continue;
         const int kk = k == M ? 0 : k, km = k == 0 ? 0 : M - k;
         const float2 a = sm[c * LP + kk + (kk >> 4)], b = sm[c * LP + km + (km >> 4)];
@@ -772,9 +781,12 @@ int launch_r_l(mm_tomo* h, bool inv, const void* src, void* dst, cudaStream_t st
         MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<grid, block, smem, st>>>((const float2*)src, (TS*)dst, h->d_twr, h->d_exr, C);
     } else {
+        constexpr int CBr = rr_cols<M>();
+        const size_t smem_r = (size_t)CBr * (M + M / 16 + 1) * sizeof(float2);
         auto kern = k_rr2c<M, TS>;
-        MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<grid, block, smem, st>>>((const TS*)src, (float2*)dst, h->d_twr, h->d_exr, C);
+        MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_r));
+        kern<<<dim3((unsigned)((C + CBr - 1) / CBr)), dim3(G, CBr), smem_r, st>>>((const TS*)src, (float2*)dst,
+                                                                                 h->d_twr, h->d_exr, C);
     }
     MM_LAUNCHED();
     return MM_OK;
