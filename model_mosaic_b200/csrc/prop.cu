@@ -112,30 +112,39 @@ __global__ void __launch_bounds__(CW * stockham::Sched<N>::G,
     stockham::pairconv<N>(sm, ad, ld, pair, st, g, tw, tw + 3 * N / 2);
 }
 
-// The column pass of the intensity chain (psi built on load) for 64-row
-// frames of width 2048, persistent and software-pipelined: each block walks
-// over (frame, 32-column group) items and loads the next item's 16
-// projection values per thread before it transforms the current one, so the
+// The column pass for 64-row frames (IN 1: psi built on load from the
+// projections; IN 0: complex input), persistent and software-pipelined: each
+// block walks over (frame, 32-column group) items and loads the next item's
+// 16 input values per thread before it transforms the current one, so the
 // loads of one item overlap the FFT of the previous (the one-item-per-block
 // form waits on its loads at the start of every item).
-template <int NXC>
-__global__ void __launch_bounds__(128, 6)
-    k_ypass_pf(const float* __restrict__ src, float2* __restrict__ dst, const float4* __restrict__ Sy,
+template <int IN>
+struct ColIn;
+template <>
+struct ColIn<0> { using T = float2; };
+template <>
+struct ColIn<1> { using T = float; };
+
+template <int IN, int NXC>
+__global__ void __launch_bounds__(128, IN == 1 ? 6 : 5)
+    k_ypass_pf(const void* __restrict__ src_v, float2* __restrict__ dst, const float4* __restrict__ Sy,
                const float2* __restrict__ tw, long items, int n_rt, float s, float ib) {
+    using T = typename ColIn<IN>::T;
     constexpr int N = 64, CW = 32, NG = 4;  // stockham::Sched<64>: G = 4 threads, first pass radix 16 over NG = 4
     static_assert(stockham::Sched<N>::G == 4 && stockham::PassShape<N, false, 0>::NG == NG &&
                       stockham::PassShape<N, false, 0>::Q == 1,
                   "first-pass layout of the 64-point line");
+    const T* __restrict__ src = static_cast<const T*>(src_v);
     const int n = NXC > 0 ? NXC : n_rt;
     extern __shared__ float2 sm[];
     const int c = threadIdx.x, g = threadIdx.y;
     const int ngroups = n / CW;
     const stockham::ColAddr<CW> ad{c};
-    float raw[16], nxt[16];
-    auto fetch = [&](long it, float (&v)[16]) {
+    T raw[16], nxt[16];
+    auto fetch = [&](long it, T (&v)[16]) {
         const long frame = it / ngroups;
         const int x = (int)(it % ngroups) * CW + c;
-        const float* base = src + frame * N * (long)n + x;
+        const T* base = src + frame * N * (long)n + x;
 #pragma unroll
         for (int i = 0; i < 16; ++i) v[i] = __ldg(base + (long)sig(g + NG * i, N) * n);
     };
@@ -148,11 +157,15 @@ __global__ void __launch_bounds__(128, 6)
         const int x = (int)(it % ngroups) * CW + c;
         const long plane = frame * N * (long)n;
         auto ld = [&](int pos) -> float2 {
-            const float ph = raw[(pos - g) / NG] * s;
-            const float at = expf(-ph * ib);
-            float sn, cs;
-            sincosf(ph, &sn, &cs);
-            return make_float2(at * cs, at * sn);
+            if constexpr (IN == 0) {
+                return raw[(pos - g) / NG];
+            } else {
+                const float ph = raw[(pos - g) / NG] * s;
+                const float at = expf(-ph * ib);
+                float sn, cs;
+                sincosf(ph, &sn, &cs);
+                return make_float2(at * cs, at * sn);
+            }
         };
         auto pair = [&](int k, float2 a, float2 b) { return pair_mix(Sy, k, a, b); };
         auto st = [&](int pos, float2 v) { dst[plane + (long)sig(pos, N) * n + x] = v; };
@@ -326,9 +339,9 @@ int launch_y(mm_prop* h, const void* src, int ntheta, const float4* S, float s, 
     constexpr int G = stockham::Sched<N>::G;
     constexpr int CW = y_cols<N>();
     const size_t smem = (size_t)stockham::ColAddr<CW>::rows(N) * CW * sizeof(float2);
-    if constexpr (N == 64 && IN == 1) {
-        if (h->n % 32 == 0) {  // 64-row frames of the intensity chain: persistent prefetching column pass
-            auto kern = h->n == 2048 ? k_ypass_pf<2048> : k_ypass_pf<0>;
+    if constexpr (N == 64) {
+        if (h->n % 32 == 0) {  // 64-row frames: persistent prefetching column pass
+            auto kern = h->n == 2048 ? k_ypass_pf<IN, 2048> : k_ypass_pf<IN, 0>;
             MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             int dev = 0, sms = 0, per_sm = 0;
             MM_CUDA(cudaGetDevice(&dev));
@@ -337,8 +350,7 @@ int launch_y(mm_prop* h, const void* src, int ntheta, const float4* S, float s, 
             const long items = (long)ntheta * (h->n / 32);
             const long blocks = std::min<long>(items, (long)sms * std::max(per_sm, 1));
             h->tm.begin(0, st);
-            kern<<<(unsigned)blocks, dim3(32, 4), smem, st>>>(static_cast<const float*>(src), h->mid, S, h->twy,
-                                                              items, h->n, s, ib);
+            kern<<<(unsigned)blocks, dim3(32, 4), smem, st>>>(src, h->mid, S, h->twy, items, h->n, s, ib);
             MM_LAUNCHED();
             h->tm.end(st, 1);
             return MM_OK;
