@@ -125,15 +125,23 @@ struct ColIn<0> { using T = float2; };
 template <>
 struct ColIn<1> { using T = float; };
 
-template <int IN, int NXC>
-__global__ void __launch_bounds__(128, IN == 1 ? 6 : 5)
+// Columns per block of the prefetching column pass (a block of CW x G
+// threads, 128 or 256).
+template <int N>
+constexpr int pf_cols() {
+    return stockham::Sched<N>::G >= 32 ? 256 / stockham::Sched<N>::G : 128 / stockham::Sched<N>::G;
+}
+
+template <int N, int IN, int NXC>
+__global__ void __launch_bounds__(pf_cols<N>() * stockham::Sched<N>::G,
+                                  (IN == 1 ? 768 : 640) / (pf_cols<N>() * stockham::Sched<N>::G))
     k_ypass_pf(const void* __restrict__ src_v, float2* __restrict__ dst, const float4* __restrict__ Sy,
                const float2* __restrict__ tw, long items, int n_rt, float s, float ib) {
     using T = typename ColIn<IN>::T;
-    constexpr int N = 64, CW = 32, NG = 4;  // stockham::Sched<64>: G = 4 threads, first pass radix 16 over NG = 4
-    static_assert(stockham::Sched<N>::G == 4 && stockham::PassShape<N, false, 0>::NG == NG &&
+    constexpr int CW = pf_cols<N>(), NG = stockham::PassShape<N, false, 0>::NG;
+    static_assert(stockham::Sched<N>::V == 16 && stockham::PassShape<N, false, 0>::RP == 16 &&
                       stockham::PassShape<N, false, 0>::Q == 1,
-                  "first-pass layout of the 64-point line");
+                  "first pass: radix 16, one group per thread");
     const T* __restrict__ src = static_cast<const T*>(src_v);
     const int n = NXC > 0 ? NXC : n_rt;
     extern __shared__ float2 sm[];
@@ -339,18 +347,20 @@ int launch_y(mm_prop* h, const void* src, int ntheta, const float4* S, float s, 
     constexpr int G = stockham::Sched<N>::G;
     constexpr int CW = y_cols<N>();
     const size_t smem = (size_t)stockham::ColAddr<CW>::rows(N) * CW * sizeof(float2);
-    if constexpr (N == 64) {
-        if (h->n % 32 == 0) {  // 64-row frames: persistent prefetching column pass
-            auto kern = h->n == 2048 ? k_ypass_pf<IN, 2048> : k_ypass_pf<IN, 0>;
+    if constexpr (stockham::Sched<N>::P2 && N >= 64 && N <= 1024) {
+        constexpr int CWp = pf_cols<N>();
+        if (h->n % CWp == 0) {  // persistent prefetching column pass
+            const size_t smem = (size_t)stockham::ColAddr<CWp>::rows(N) * CWp * sizeof(float2);
+            auto kern = h->n == 2048 ? k_ypass_pf<N, IN, 2048> : k_ypass_pf<N, IN, 0>;
             MM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             int dev = 0, sms = 0, per_sm = 0;
             MM_CUDA(cudaGetDevice(&dev));
             MM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-            MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem));
-            const long items = (long)ntheta * (h->n / 32);
+            MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, CWp * G, smem));
+            const long items = (long)ntheta * (h->n / CWp);
             const long blocks = std::min<long>(items, (long)sms * std::max(per_sm, 1));
             h->tm.begin(0, st);
-            kern<<<(unsigned)blocks, dim3(32, 4), smem, st>>>(src, h->mid, S, h->twy, items, h->n, s, ib);
+            kern<<<(unsigned)blocks, dim3(CWp, G), smem, st>>>(src, h->mid, S, h->twy, items, h->n, s, ib);
             MM_LAUNCHED();
             h->tm.end(st, 1);
             return MM_OK;
