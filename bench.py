@@ -305,7 +305,8 @@ def run_ours(args, w, rank, world, local_rank):
     achieved = alg[top] / (t_launch * 1e-3) / 1e9
     col_kernel = "k_col_l2" if (n == 2048 and nz % 8 == 0) else "k_col_fft"   # tomo_col.cu covers 2n = 4096
     kname = {"gather": "k_gather", "pad_phi": "k_xfwd", "y_fft": col_kernel, "r_c2r": "k_rc2r",
-             "y_pass": "k_ypass", "x_pass": "k_xpass"}[top]
+             "y_pass": "k_ypass_pf" if (nz & (nz - 1)) == 0 and 64 <= nz <= 1024 else "k_ypass",
+             "x_pass": "k_xpass"}[top]
     traffic = profile_traffic(args.workload, kname)
     # the step's algorithmic bytes as the hot-path scope defines them: R's
     # B_R = 4V + 16Hc + 16H + 4S and D's B_D = 24P (Hc = nz n (n+1))
