@@ -134,7 +134,7 @@ constexpr int pf_cols() {
 
 template <int N, int IN, int NXC>
 __global__ void __launch_bounds__(pf_cols<N>() * stockham::Sched<N>::G,
-                                  (IN == 1 ? 768 : 640) / (pf_cols<N>() * stockham::Sched<N>::G))
+                                  (IN == 1 ? 896 : 640) / (pf_cols<N>() * stockham::Sched<N>::G))
     k_ypass_pf(const void* __restrict__ src_v, float2* __restrict__ dst, const float4* __restrict__ Sy,
                const float2* __restrict__ tw, long items, int n_rt, float s, float ib) {
     using T = typename ColIn<IN>::T;
