@@ -130,8 +130,7 @@ def tune_classes(specs, wavelength, voxelsize, distance, *, tol=None, device=Non
             T = int(np.median([a for a, _ in members]))
             nz = max(z for _, z in members)
             errs = estimate_errors(n, dev, candidates=candidates)
-            lim = errs[REFERENCE] if (tol is None and REFERENCE in errs) else (tol if tol is not None else np.inf)
-            ok = [(float(e), int(m)) for e, m in candidates if errs[(e, m)] <= lim * (1 + 1e-6)]
+            lim, ok = admissible(errs, tol, candidates)
             key = f"{dname}|n={n}|nz={nz}|T={T}|tol={'ref' if tol is None else f'{tol:.3g}'}"
             hit = store.get(key)
             if hit and (float(hit["choice"][0]), int(hit["choice"][1])) in ok:
@@ -147,6 +146,17 @@ def tune_classes(specs, wavelength, voxelsize, distance, *, tol=None, device=Non
     if cache:
         _save(cache, store)
     return {"params": params, "report": report}
+
+
+def admissible(errs: dict, tol, candidates=CANDIDATES):
+    """(limit, [(eps, m) ...]): the candidates whose estimated error is within
+    ``tol`` -- by default the reference setting's own error, so that the
+    default never picks a less accurate pair than the reference's."""
+    if tol is None:
+        lim = errs[REFERENCE] if REFERENCE in errs else np.inf
+    else:
+        lim = float(tol)
+    return lim, [(float(e), int(m)) for e, m in candidates if errs[(e, m)] <= lim * (1 + 1e-6)]
 
 
 def batch_signature(specs) -> str:

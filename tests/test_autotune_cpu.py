@@ -31,3 +31,13 @@ def test_batch_signature():
     assert autotune.batch_signature(a) == autotune.batch_signature(b)           # nz defaults to 16
     assert autotune.batch_signature(a) != autotune.batch_signature(a[::-1])
     assert autotune.batch_signature(a) != autotune.batch_signature([a[0], dict(n=768, theta=th(401))])
+
+
+def test_admissible_rule():
+    errs = {(1e-2, 3): 4.07e-3, (1e-3, 4): 2.73e-4, (1e-5, 6): 0.0}
+    lim, ok = autotune.admissible(errs, None)
+    assert lim == errs[(1e-3, 4)] and ok == [(1e-3, 4), (1e-5, 6)]      # default: as accurate as the reference
+    lim, ok = autotune.admissible(errs, 1e-2)
+    assert ok == [(1e-2, 3), (1e-3, 4), (1e-5, 6)]
+    lim, ok = autotune.admissible(errs, 1e-4)
+    assert ok == [(1e-5, 6)]
