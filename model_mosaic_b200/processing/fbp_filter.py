@@ -9,9 +9,9 @@ Same constructor and methods as the reference class (processing/fbp_filter.py:38
 
 Each row of n samples is edge-replicated to 4n, multiplied in frequency by the
 weights and cropped back to n (processing/fbp_filter.py:182-191).  The work
-runs in ``libmosaic.so``: for 4n a power of two up to 8192 one fused kernel per
-two rows, in place and without scratch; other n through cuFFT, batch_chunk rows
-at a time.  The weights are host-side FP64 arithmetic, as in the reference
+runs in ``libmosaic.so``: for 4n a power of two up to 8192 or 3 * 2^k up to
+12288 one fused kernel per two rows, in place and without scratch; other n
+through cuFFT, batch_chunk rows at a time.  The weights are host-side FP64 arithmetic, as in the reference
 (NumPy here), copied to the device once per filter name.  Inputs may be torch
 CUDA tensors or ``__cuda_array_interface__`` arrays (cupy); `filter` writes
 into the caller's array as the reference does.

@@ -9,7 +9,8 @@ phase = -log(clip(irfft2(H * rfft2(I)), 1e-6)) per frame with
 H = alpha / (lambda z (kx^2 + ky^2) / (4 pi) + alpha).  The filter table is
 built here exactly as the reference builds it (float32 arithmetic on the
 fftfreq x rfftfreq grid, :46-53); the transform runs in ``libmosaic.so`` (three
-fused passes for power-of-two sizes up to 4096, cuFFT otherwise).  Inputs may
+fused passes for sizes 2^k up to 4096 and 3 * 2^k in [96, 3072], cuFFT
+otherwise).  Inputs may
 be torch CUDA tensors, ``__cuda_array_interface__`` arrays or numpy arrays;
 the result comes back as the same kind.
 """

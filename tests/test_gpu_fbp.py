@@ -1,5 +1,5 @@
-"""GPU FBP filter (fused Stockham kernel for 4n a power of two up to 8192,
-cuFFT otherwise) against the reference's FBPFilter outputs and the FP64
+"""GPU FBP filter (fused Stockham kernel for 4n a power of two up to 8192 or
+3 * 2^k up to 12288, cuFFT otherwise) against the reference's FBPFilter outputs and the FP64
 oracle: relative L2 <= 1e-5, in place, the reference's chunking and host
 variants, and the filter followed by RT as step8_fbp.py does."""
 import os

@@ -1,4 +1,4 @@
-"""GPU Paganin retrieval (three fused passes for power-of-two sizes, cuFFT
+"""GPU Paganin retrieval (three fused passes for 2^k and 3 * 2^k sizes, cuFFT
 otherwise) against the reference's own Paganin outputs
 (tests/golden/make_golden_paganin.py) and the FP64 oracle: relative L2 <= 1e-5;
 2-D input, batches smaller than ntheta, PaganinLarge's chunk validation

@@ -56,8 +56,10 @@ def test_D_large_and_validation(gold):
 
 @pytest.mark.parametrize("n,nz,nt", [(64, 32, 3), (256, 64, 5), (2048, 64, 2), (128, 8, 4), (8, 2, 2),
                                       (16, 4, 3), (2, 16, 2), (512, 128, 2), (32, 2048, 1),
-                                      # general sizes (cuFFT 2-D path): odd, non-power-of-two, mixed
-                                      (12, 6, 3), (5, 7, 2), (96, 64, 3), (64, 48, 2), (768, 16, 2)])
+                                      # general sizes (cuFFT 2-D path): odd, other lengths, mixed
+                                      (12, 6, 3), (5, 7, 2), (64, 48, 2),
+                                      # 3 * 2^k lengths on the native kernels
+                                      (96, 64, 3), (768, 16, 2)])
 def test_D_DT_vs_oracle_and_adjoint(n, nz, nt):
     from model_mosaic_b200.processing.propagation import Propagation
     wl, vs, dist = 4.133e-11, 0.69e-6, [0.12, 0.02]
